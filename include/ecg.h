@@ -1,0 +1,379 @@
+/*
+ * ecg.h -- C ABI of the B200 (sm_100a) euler_compare hot path.
+ *
+ * The reference keeps its hot path as internal C++ functions inside one
+ * translation unit (amrex/apps/euler_compare/src/euler_compare_app.cpp:41-62);
+ * each entry point below replaces one of those calls so that the AMReX driver
+ * (amrex/apps/euler_compare/src/euler_compare/app/driver_main.hpp) can keep its
+ * call sites, ParmParse selectors and MultiFab layout.  Plain C types only: no
+ * CUDA or torch types cross this boundary.
+ *
+ * Ownership: a context owns every device buffer (state, scratch, Krylov basis).
+ * The host MultiFab is copied only by ecg_upload_state / ecg_download_state.
+ * Threading: one context per host thread; a context is not internally
+ * thread-safe.  Errors: every call returns an ecg_status; nothing throws
+ * across the ABI.  IMEX solver outcomes (the reference's solver_status
+ * strings) are reported in ecg_imex_diag.solver_status, as the reference
+ * reports them in ImexStepDiagnostics, and do not make the call fail.
+ */
+#ifndef ECG_H
+#define ECG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ECG_ABI_VERSION 1
+
+typedef enum ecg_status {
+  ECG_OK = 0,
+  ECG_ERR_BAD_ARG = 1,      /* invalid pointer, size or option */
+  ECG_ERR_CUDA = 2,         /* a CUDA runtime call failed; see ecg_last_error */
+  ECG_ERR_TIMEOUT = 3,      /* a bounded device-side wait gave up */
+  ECG_ERR_NO_DEVICE = 4,    /* no usable sm_100 device */
+  ECG_ERR_UNSUPPORTED = 5,  /* configuration outside the rebuilt hot path */
+  ECG_ERR_NOT_READY = 6     /* state not uploaded yet */
+} ecg_status;
+
+/* Mirrors ProblemKind (core/solver_types.hpp:2-10), same order. */
+typedef enum ecg_problem {
+  ECG_PROBLEM_ADVECTION_BLOB = 0,
+  ECG_PROBLEM_TORO1 = 1,
+  ECG_PROBLEM_GRESHO_VORTEX = 2,
+  ECG_PROBLEM_RIEMANN_QUADRANT = 3,
+  ECG_PROBLEM_ISENTROPIC_VORTEX = 4,
+  ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D = 5,
+  ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_CYLINDRICAL = 6
+} ecg_problem;
+
+/* Mirrors RiemannKind (core/solver_types.hpp:11). */
+typedef enum ecg_riemann {
+  ECG_RIEMANN_RUSANOV = 0,
+  ECG_RIEMANN_HLLC = 1,
+  ECG_RIEMANN_LOWMACH_HLLC = 2,
+  ECG_RIEMANN_XIE_AM_HLLC_P = 3
+} ecg_riemann;
+
+/* Mirrors MethodKind (core/solver_types.hpp:12). */
+typedef enum ecg_method { ECG_METHOD_EXPLICIT = 0, ECG_METHOD_IMEX = 1 } ecg_method;
+
+/* Mirrors SlopeLimiterKind (core/solver_types.hpp:14). */
+typedef enum ecg_limiter {
+  ECG_LIMITER_MINMOD = 0,
+  ECG_LIMITER_MC = 1,
+  ECG_LIMITER_VANLEER = 2
+} ecg_limiter;
+
+/* RunConfig::field_boundary string (core/run_config.hpp:48). */
+typedef enum ecg_field_boundary {
+  ECG_FIELD_BOUNDARY_OUTFLOW = 0,
+  ECG_FIELD_BOUNDARY_EXACT_DIRICHLET = 1
+} ecg_field_boundary;
+
+/*
+ * Numeric mirror of RunConfig (core/run_config.hpp:2-55).  String selectors
+ * become the enums above.  ecg_default_run_config fills RunConfig's defaults.
+ */
+typedef struct ecg_run_config {
+  int32_t n_cell[2];
+  int32_t is_periodic[2];
+  double prob_lo[2];
+  double prob_hi[2];
+  int32_t max_step;
+  int32_t spatial_order;
+  int32_t toro_test;
+  int32_t problem;         /* ecg_problem */
+  int32_t riemann;         /* ecg_riemann */
+  int32_t method;          /* ecg_method */
+  int32_t slope_limiter;   /* ecg_limiter */
+  int32_t field_boundary;  /* ecg_field_boundary */
+  double stop_time;
+  double gamma;
+  double cfl;
+  double imex_cfl;
+  double imex_acoustic_cfl_cap;
+  double imex_solver_tol;
+  double velocity_x;
+  double velocity_y;
+  double density_inner;
+  double density_outer;
+  double pressure;
+  double mach;
+  double blob_cx;
+  double blob_cy;
+  double blob_radius;
+  double vortex_cx;
+  double vortex_cy;
+  double isentropic_vortex_strength;
+  double riemann_interface_x;
+  double riemann_interface_y;
+  int32_t imex_solver_max_iter;
+  int32_t imex_acoustic_startup;
+  int32_t imex_picard_iterations;
+  int32_t imex_picard_extra_iterations;
+} ecg_run_config;
+
+/* Arithmetic contract of the FP64 stencil kernels. */
+typedef enum ecg_arith {
+  /* Default: nvcc contracts a*b+c into FMA.  Per step within 1e-12 relative
+   * of the reference CPU build. */
+  ECG_ARITH_FAST = 0,
+  /* No contraction, IEEE division and square root, the reference's operation
+   * order: bit-identical to the reference CPU build (gcc, x86-64, no FMA). */
+  ECG_ARITH_EXACT = 1
+} ecg_arith;
+
+/* Precision of the IMEX pressure solve. */
+typedef enum ecg_imex_precision {
+  ECG_IMEX_FP64 = 0,   /* all-FP64 GMRES */
+  ECG_IMEX_MIXED = 1   /* FP32 inner GMRES, FP64 residual + iterative refinement */
+} ecg_imex_precision;
+
+typedef struct ecg_gpu_options {
+  int32_t device;           /* CUDA device ordinal */
+  int32_t arith;            /* ecg_arith */
+  int32_t imex_precision;   /* ecg_imex_precision */
+  int32_t mixed_inner_max_iter;  /* FP32 inner iterations per refinement sweep */
+  double mixed_inner_rtol;       /* FP32 inner relative residual target */
+  int32_t mixed_max_refinements; /* outer FP64 refinement sweeps */
+  int32_t tile_x;           /* explicit-kernel tile (0 = autotuned default) */
+  int32_t tile_y;
+  void* stream;             /* cudaStream_t to run on, NULL = context-owned stream */
+} ecg_gpu_options;
+
+/* Diagnostics (core/basic_diagnostics.hpp:3-7). */
+typedef struct ecg_diagnostics {
+  double rho_min;
+  double pressure_min;
+  int32_t nonfinite_count;
+} ecg_diagnostics;
+
+/* AdmissibilityDiagnostics (core/basic_diagnostics.hpp:9-17). */
+typedef struct ecg_admissibility {
+  double rho_min;
+  double pressure_min;
+  double internal_energy_min;
+  int32_t nonfinite_count;
+  int32_t density_failure_count;
+  int32_t pressure_failure_count;
+  int32_t internal_energy_failure_count;
+} ecg_admissibility;
+
+/* ImexTimeStepDiagnostics (core/problem_metrics.hpp:14-19). */
+typedef struct ecg_imex_timestep_diag {
+  double material_rate_max;
+  double acoustic_rate_max;
+  int32_t acoustic_startup_used;
+  int32_t acoustic_cap_used;
+} ecg_imex_timestep_diag;
+
+/* ImexStepDiagnostics solver_status strings (imex/imex_source_map_step.hpp:398-567). */
+typedef enum ecg_solver_status {
+  ECG_SOLVER_NOT_RUN = 0,
+  ECG_SOLVER_CONVERGED_ABSOLUTE = 1,
+  ECG_SOLVER_CONVERGED_RELATIVE = 2,
+  ECG_SOLVER_LINEAR_SOLVE_NOT_CONVERGED = 3,
+  ECG_SOLVER_GMRES_BREAKDOWN_NOT_CONVERGED = 4,
+  ECG_SOLVER_LINEAR_RESIDUAL_NONFINITE = 5,
+  ECG_SOLVER_SOURCE_MAP_PRESSURE_ROW_NONFINITE = 6,
+  ECG_SOLVER_SOURCE_MAP_LAGGED_MOMENTUM_NONFINITE = 7,
+  ECG_SOLVER_DENSITY_DENOMINATOR_FLOOR_USED = 8,
+  ECG_SOLVER_UNSUPPORTED_MPI = 9
+} ecg_solver_status;
+
+/*
+ * Numeric fields of ImexStepDiagnostics (core/imex_diagnostics.hpp:5-171)
+ * that euler_imex_bdltv20_o1_source_map_picard_one_step fills
+ * (imex/imex_source_map_step.hpp:300-616).  The label strings of that record
+ * are constants of the method and are not repeated here.
+ */
+typedef struct ecg_imex_diag {
+  int32_t solver_status;              /* ecg_solver_status */
+  int32_t linear_solver_status_last;  /* ecg_solver_status */
+  int32_t solver_iterations;          /* summed over Picard solves */
+  int32_t picard_pressure_solves_used;
+  int32_t source_picard_iterations_used;
+  int32_t kinetic_lag_update_count;
+  int32_t kinetic_lag_nonfinite_count;
+  int32_t pressure_matrix_rows;
+  int32_t pressure_matrix_nonzeros;
+  int32_t pressure_matrix_max_row_width;
+  int32_t density_denominator_floor_count;
+  int32_t nonfinite_count;
+  int32_t positivity_failure_count;
+  int32_t face_enthalpy_denominator_guard_count;
+  int32_t face_enthalpy_nonfinite_count;
+  int32_t energy_flux_nonfinite_count;
+  int32_t gmres_inner_iterations;     /* mixed precision: FP32 iterations (not in the reference) */
+  int32_t gmres_refinements;          /* mixed precision: FP64 refinement sweeps (not in the reference) */
+  double solver_initial_residual;
+  double solver_initial_rhs_norm;
+  double solver_residual;
+  double solver_relative_residual;
+  double pressure_linear_residual_linf;
+  double pressure_linear_residual_relative_linf;
+  double kinetic_jacobian_abs_max;
+  double pressure_matrix_symmetry_linf;
+  double pressure_picard_delta_linf;
+  double source_picard_delta_l2_relative_to_pmax;
+  double pressure_energy_residual_before_linf;
+  double coupled_residual_l1_final;
+  double coupled_residual_linf_final;
+  double coupled_residual_relative_linf_final;
+  double pressure_energy_residual_l1;
+  double pressure_energy_residual_linf;
+  double pressure_energy_residual_relative_linf;
+  double rho_min;
+  double pressure_min;
+  double internal_energy_min;
+  double trial_density_min;
+  double solved_pressure_min;
+  double solved_pressure_max;
+  double eos_pressure_min;
+  double eos_pressure_max;
+  double internal_energy_max;
+  double momentum_correction_linf;
+  double energy_correction_linf;
+  double energy_flux_linf;
+  double energy_flux_divergence_linf;
+  double eq78_divergence_linf;
+  double eq78_divergence_scaled_linf;
+  double energy_closeout_delta_l1;
+  double energy_closeout_delta_linf;
+} ecg_imex_diag;
+
+/* Result of a device-resident time loop (driver_main.hpp:224-333). */
+typedef struct ecg_run_result {
+  int32_t steps;
+  int32_t failed;               /* 0 = ok */
+  int32_t failure_code;         /* ecg_failure_* below */
+  int32_t hllc_degenerate_star_count;
+  int32_t imex_solver_iterations_max;
+  double time;
+  double dt_min;
+  double dt_max;
+  double dt_sum;
+  ecg_diagnostics diagnostics;  /* after the last step */
+} ecg_run_result;
+
+/* Failure categories of the driver loop (driver_main.hpp:216-340). */
+enum {
+  ECG_FAILURE_NONE = 0,
+  ECG_FAILURE_NONFINITE_STATE = 1,
+  ECG_FAILURE_NONPOSITIVE_DENSITY = 2,
+  ECG_FAILURE_NONPOSITIVE_PRESSURE = 3,
+  ECG_FAILURE_INVALID_TIME_STEP = 4,
+  ECG_FAILURE_IMEX_SOLVER = 5,
+  ECG_FAILURE_MAX_STEP_BEFORE_STOP_TIME = 6
+};
+
+typedef struct ecg_ctx ecg_ctx;
+
+/* ---- library ---------------------------------------------------------- */
+int32_t ecg_abi_version(void);
+const char* ecg_status_str(ecg_status s);
+/* The reference's exact solver_status string for an ecg_solver_status. */
+const char* ecg_solver_status_str(int32_t solver_status);
+/* RunConfig defaults (core/run_config.hpp:2-55). */
+void ecg_default_run_config(ecg_run_config* cfg);
+void ecg_default_gpu_options(ecg_gpu_options* opt);
+
+/* ---- context ---------------------------------------------------------- */
+/* Validates cfg as read_config does for the rebuilt path
+ * (core/config_reader.hpp:123-324) and allocates the device state. */
+ecg_status ecg_create(ecg_ctx** out, const ecg_run_config* cfg, const ecg_gpu_options* opt);
+void ecg_destroy(ecg_ctx* ctx);
+const char* ecg_last_error(const ecg_ctx* ctx);
+
+/*
+ * State exchange with one AMReX FArrayBox / Array4 covering the domain.
+ * Element (i, j, comp) lives at base[(i - lo_x) + (j - lo_y) * jstride + comp * nstride]
+ * (AMReX_Array4.H), comp in {Rho, Mx, My, E} (euler_compare_app.cpp:47).
+ * Only the valid cells [0, nx) x [0, ny) are copied; ghost cells are derived
+ * on the device from the boundary conditions.
+ */
+ecg_status ecg_upload_state(ecg_ctx* ctx, const double* base, int32_t lo_x, int32_t lo_y,
+                            int64_t jstride, int64_t nstride);
+ecg_status ecg_download_state(ecg_ctx* ctx, double* base, int32_t lo_x, int32_t lo_y,
+                              int64_t jstride, int64_t nstride);
+/* Same with base in device memory (e.g. a torch CUDA tensor). */
+ecg_status ecg_upload_state_device(ecg_ctx* ctx, const double* base, int32_t lo_x, int32_t lo_y,
+                                   int64_t jstride, int64_t nstride);
+ecg_status ecg_download_state_device(ecg_ctx* ctx, double* base, int32_t lo_x, int32_t lo_y,
+                                     int64_t jstride, int64_t nstride);
+/* Fills the whole ghosted box [-2, nx+2) x [-2, ny+2) (4 planes, jstride
+ * nx+4, nstride (nx+4)(ny+4)) as fill_problem_ghosts does
+ * (problems/boundary_conditions.hpp:202-219). */
+ecg_status ecg_fill_problem_ghosts(ecg_ctx* ctx, double time, double* ghosted_host);
+
+/* Synchronises the context's stream. */
+ecg_status ecg_synchronize(ecg_ctx* ctx);
+
+/* ---- hot path --------------------------------------------------------- */
+/* euler_fv_one_step (numerics/explicit_update.hpp:58-102): one forward-Euler
+ * MUSCL + Riemann-flux update of the device state.  Returns the
+ * count_hllc_degenerate_star_states value (explicit_update.hpp:2-56) through
+ * hllc_degenerate_count when non-NULL. */
+ecg_status ecg_euler_fv_one_step(ecg_ctx* ctx, double dt, double time, int32_t* hllc_degenerate_count);
+/* compute_euler_dt (numerics/diagnostic_metrics_timestep.hpp:227-260). */
+ecg_status ecg_compute_euler_dt(ecg_ctx* ctx, double time, double* dt);
+/* compute_imex_dt (numerics/diagnostic_metrics_timestep.hpp:272-326). */
+ecg_status ecg_compute_imex_dt(ecg_ctx* ctx, double time, double* dt, ecg_imex_timestep_diag* diag);
+/* compute_diagnostics (numerics/diagnostic_metrics_timestep.hpp:18-47). */
+ecg_status ecg_compute_diagnostics(ecg_ctx* ctx, ecg_diagnostics* out);
+/* compute_admissibility_diagnostics (numerics/diagnostic_metrics_timestep.hpp:49-111). */
+ecg_status ecg_compute_admissibility_diagnostics(ecg_ctx* ctx, ecg_admissibility* out);
+/* euler_imex_bdltv20_o1_source_map_picard_one_step
+ * (imex/imex_source_map_step.hpp:300-616): the IMEX T1/S2 BDLTV20 step with
+ * the GMRES pressure solve.  The state is updated only when the step
+ * succeeds, as in the reference. */
+ecg_status ecg_imex_step(ecg_ctx* ctx, double dt, ecg_imex_diag* out);
+/* The driver's time loop (app/driver_main.hpp:224-333) kept on the device:
+ * dt, step and fail-fast diagnostics per step, no host round trip for the
+ * explicit method. */
+ecg_status ecg_run(ecg_ctx* ctx, int32_t max_step, double stop_time, ecg_run_result* out);
+
+/* ---- adjoint of the explicit step --------------------------------------- */
+/* Vector-Jacobian product of U1 = euler_fv_one_step(U0; dt) with dt held
+ * fixed: gU0 = (dU1/dU0)^T gU1.  All arrays are device memory holding 4
+ * planes of nx*ny doubles (component-major, i fastest).  Boundary conditions
+ * are the context's.  No counterpart in the reference (its code has no
+ * adjoint). */
+ecg_status ecg_explicit_step_vjp_device(ecg_ctx* ctx, const double* u0, double dt,
+                                        const double* g_u1, double* g_u0);
+/* Forward step on caller-provided device planes (same layout), used by the
+ * checkpointed adjoint: u1 = euler_fv_one_step(u0; dt). */
+ecg_status ecg_explicit_step_device(ecg_ctx* ctx, const double* u0, double dt, double* u1);
+
+/* ---- batched independent solves ----------------------------------------- */
+/* Many explicit O2 solves of uneven grid sizes advanced together by one
+ * persistent launch per step (captured in a CUDA graph).  Each solve keeps
+ * its own dt (compute_euler_dt per solve).  No counterpart in the reference,
+ * which runs one solve per process. */
+typedef struct ecg_batch ecg_batch;
+typedef struct ecg_batch_result {
+  int32_t steps;
+  int32_t failed;
+  int32_t hllc_degenerate_star_count;
+  int32_t pad;
+  double time;
+  ecg_diagnostics diagnostics;
+} ecg_batch_result;
+ecg_status ecg_batch_create(ecg_batch** out, int32_t nsolve, const ecg_run_config* cfgs,
+                            const ecg_gpu_options* opt);
+void ecg_batch_destroy(ecg_batch* b);
+ecg_status ecg_batch_upload(ecg_batch* b, int32_t solve, const double* base, int32_t lo_x, int32_t lo_y,
+                            int64_t jstride, int64_t nstride);
+ecg_status ecg_batch_download(ecg_batch* b, int32_t solve, double* base, int32_t lo_x, int32_t lo_y,
+                              int64_t jstride, int64_t nstride);
+/* Advances every solve by `steps` steps (each solve stops at its stop_time). */
+ecg_status ecg_batch_run(ecg_batch* b, int32_t steps, ecg_batch_result* per_solve);
+const char* ecg_batch_last_error(const ecg_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ECG_H */

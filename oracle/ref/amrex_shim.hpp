@@ -1,0 +1,368 @@
+// Minimal single-box stand-in for the parts of AMReX that the euler_compare
+// hot-path headers use.  TEST INFRASTRUCTURE ONLY: it lets the reference's own
+// numerics headers (amrex/apps/euler_compare/src/euler_compare/**) compile with
+// plain g++ into oracle/_ref/, so the CPU oracle is the reference's code itself.
+//
+// Semantics follow AMReX where the numerics can observe them:
+//  * Array4 indexing p[(i-lo.x) + (j-lo.y)*jstride + n*nstride]
+//    (external/AMReX/Src/Base/AMReX_Array4.H).
+//  * Geometry cell size dx = (prob_hi - prob_lo) / n  (AMReX_Geometry.cpp:527).
+//  * ReduceOpSum/Min/Max init 0 / numeric_limits::max() / lowest() and
+//    local_update d+=s, d=min(d,s), d=max(d,s)  (AMReX_Reduce.H:283-380);
+//    CPU eval visits cells k, j, i with i fastest (AMReX_Reduce.H:1380-1395).
+//  * amrex::min/max are std::min/std::max (AMReX_Algorithm.H:20-56).
+//  * FillBoundary(periodicity) fills a ghost cell iff its periodic image lies
+//    in the valid domain (single box covering the domain).
+// Everything is one box: the reference's numerics do not depend on the box
+// decomposition except through the order of floating-point sums.
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <limits>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#define AMREX_SPACEDIM 2
+#define AMREX_GPU_HOST_DEVICE
+#define AMREX_GPU_DEVICE
+#define AMREX_FORCE_INLINE inline
+#define AMREX_D_DECL(a, b, c) a, b
+#define BL_PROFILE(x)
+
+namespace amrex {
+
+using Real = double;
+using Long = long long;
+template <class T>
+using Vector = std::vector<T>;
+template <class T, std::size_t N>
+using Array = std::array<T, N>;
+
+template <class T, int N>
+struct GpuArray {
+  T arr[N];
+  const T& operator[](int i) const noexcept { return arr[i]; }
+  T& operator[](int i) noexcept { return arr[i]; }
+};
+
+template <class T>
+inline const T& min(const T& a, const T& b) noexcept { return std::min(a, b); }
+template <class T, class... Ts>
+inline const T& min(const T& a, const T& b, const Ts&... c) noexcept { return min(min(a, b), c...); }
+template <class T>
+inline const T& max(const T& a, const T& b) noexcept { return std::max(a, b); }
+template <class T, class... Ts>
+inline const T& max(const T& a, const T& b, const Ts&... c) noexcept { return max(max(a, b), c...); }
+
+[[noreturn]] inline void Abort(const std::string& msg) { throw std::runtime_error(msg); }
+
+// Print: output is discarded (the oracle compares numbers, not text).
+// iostreams are kept out of every path the oracle calls.
+struct Print {
+  template <class T>
+  Print& operator<<(const T&) { return *this; }
+};
+
+struct Dim3 { int x, y, z; };
+
+struct IntVect {
+  int v[2] = {0, 0};
+  IntVect() = default;
+  IntVect(int a, int b) { v[0] = a; v[1] = b; }
+  int operator[](int d) const noexcept { return v[d]; }
+  int& operator[](int d) noexcept { return v[d]; }
+};
+
+struct Box {
+  IntVect lo, hi;
+  Box() = default;
+  Box(const IntVect& l, const IntVect& h) : lo(l), hi(h) {}
+  const IntVect& smallEnd() const noexcept { return lo; }
+  const IntVect& bigEnd() const noexcept { return hi; }
+  int smallEnd(int d) const noexcept { return lo[d]; }
+  int bigEnd(int d) const noexcept { return hi[d]; }
+  int length(int d) const noexcept { return hi[d] - lo[d] + 1; }
+  Box grow(const IntVect& g) const { return Box(IntVect(lo[0] - g[0], lo[1] - g[1]), IntVect(hi[0] + g[0], hi[1] + g[1])); }
+  bool contains(int i, int j) const noexcept { return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1]; }
+};
+inline Dim3 lbound(const Box& b) noexcept { return Dim3{b.lo[0], b.lo[1], 0}; }
+inline Dim3 ubound(const Box& b) noexcept { return Dim3{b.hi[0], b.hi[1], 0}; }
+
+template <class T>
+struct Array4 {
+  T* p = nullptr;
+  Long jstride = 0;
+  Long nstride = 0;
+  Dim3 begin{0, 0, 0};
+  int ncomp = 0;
+  Array4() = default;
+  Array4(T* p_, Long js, Long ns, Dim3 b, int nc) : p(p_), jstride(js), nstride(ns), begin(b), ncomp(nc) {}
+  template <class U, class = std::enable_if_t<std::is_same<std::add_const_t<U>, T>::value && !std::is_same<U, T>::value>>
+  Array4(const Array4<U>& o) : p(o.p), jstride(o.jstride), nstride(o.nstride), begin(o.begin), ncomp(o.ncomp) {}
+  T& operator()(int i, int j, int) const noexcept { return p[(i - begin.x) + (j - begin.y) * jstride]; }
+  T& operator()(int i, int j, int, int n) const noexcept {
+    return p[(i - begin.x) + (j - begin.y) * jstride + n * nstride];
+  }
+};
+
+struct RealBox {
+  Real xlo[2], xhi[2];
+  RealBox(const Real* lo, const Real* hi) { for (int d = 0; d < 2; ++d) { xlo[d] = lo[d]; xhi[d] = hi[d]; } }
+  Real length(int d) const noexcept { return xhi[d] - xlo[d]; }
+};
+
+struct CoordSys { enum CoordType { cartesian = 0 }; };
+
+struct Periodicity { int period[2] = {0, 0}; };
+
+struct Geometry {
+  Box domain;
+  Real plo[2] = {0, 0}, phi[2] = {1, 1}, dx[2] = {1, 1};
+  int per[2] = {0, 0};
+  Geometry() = default;
+  Geometry(const Box& dom, const RealBox* rb, int, const int* is_per) : domain(dom) {
+    for (int k = 0; k < 2; ++k) {
+      plo[k] = rb->xlo[k];
+      phi[k] = rb->xhi[k];
+      dx[k] = rb->length(k) / (Real(domain.length(k)));
+      per[k] = is_per[k];
+    }
+  }
+  GpuArray<Real, 2> CellSizeArray() const noexcept { return GpuArray<Real, 2>{{dx[0], dx[1]}}; }
+  GpuArray<Real, 2> ProbLoArray() const noexcept { return GpuArray<Real, 2>{{plo[0], plo[1]}}; }
+  GpuArray<Real, 2> ProbHiArray() const noexcept { return GpuArray<Real, 2>{{phi[0], phi[1]}}; }
+  const Box& Domain() const noexcept { return domain; }
+  bool isPeriodic(int d) const noexcept { return per[d] != 0; }
+  Periodicity periodicity() const noexcept {
+    Periodicity pr;
+    for (int d = 0; d < 2; ++d) { pr.period[d] = per[d] ? domain.length(d) : 0; }
+    return pr;
+  }
+};
+
+struct BoxArray {
+  Box box;
+  BoxArray() = default;
+  explicit BoxArray(const Box& b) : box(b) {}
+  void maxSize(int) {}
+};
+struct DistributionMapping {
+  DistributionMapping() = default;
+  explicit DistributionMapping(const BoxArray&) {}
+};
+
+class MFIter;
+
+class MultiFab {
+ public:
+  BoxArray ba;
+  Box valid, grown;
+  int ncomp = 0, ng = 0;
+  Long jstride = 0, nstride = 0;
+  std::vector<Real> data;
+
+  MultiFab() = default;
+  MultiFab(const BoxArray& ba_, const DistributionMapping&, int nc, int ngrow)
+      : ba(ba_), valid(ba_.box), ncomp(nc), ng(ngrow) {
+    grown = valid.grow(IntVect(ng, ng));
+    jstride = grown.length(0);
+    nstride = jstride * grown.length(1);
+    data.assign(static_cast<std::size_t>(nstride * ncomp), 0.0);
+  }
+  Array4<Real> array(const MFIter&) { return Array4<Real>(data.data(), jstride, nstride, lbound(grown), ncomp); }
+  Array4<const Real> array(const MFIter&) const { return const_array_impl(); }
+  Array4<const Real> const_array(const MFIter&) const { return const_array_impl(); }
+  Array4<Real> arr() { return Array4<Real>(data.data(), jstride, nstride, lbound(grown), ncomp); }
+  Array4<const Real> const_array_impl() const {
+    return Array4<const Real>(data.data(), jstride, nstride, lbound(grown), ncomp);
+  }
+  IntVect nGrowVect() const noexcept { return IntVect(ng, ng); }
+  int nComp() const noexcept { return ncomp; }
+  const BoxArray& boxArray() const noexcept { return ba; }
+  DistributionMapping DistributionMap() const { return DistributionMapping(ba); }
+
+  void FillBoundary(const Periodicity& per) {
+    auto a = arr();
+    const int nx = valid.length(0), ny = valid.length(1);
+    for (int n = 0; n < ncomp; ++n) {
+      for (int j = grown.lo[1]; j <= grown.hi[1]; ++j) {
+        for (int i = grown.lo[0]; i <= grown.hi[0]; ++i) {
+          if (valid.contains(i, j)) { continue; }
+          int ii = i, jj = j;
+          if (per.period[0] != 0) { ii = ((i - valid.lo[0]) % nx + nx) % nx + valid.lo[0]; }
+          if (per.period[1] != 0) { jj = ((j - valid.lo[1]) % ny + ny) % ny + valid.lo[1]; }
+          if (valid.contains(ii, jj)) { a(i, j, 0, n) = a(ii, jj, 0, n); }
+        }
+      }
+    }
+  }
+  Real sum(int comp) const {
+    auto a = const_array_impl();
+    Real s = 0.0;
+    for (int j = valid.lo[1]; j <= valid.hi[1]; ++j) {
+      for (int i = valid.lo[0]; i <= valid.hi[0]; ++i) { s += a(i, j, 0, comp); }
+    }
+    return s;
+  }
+  static void Copy(MultiFab& dst, const MultiFab& src, int scomp, int dcomp, int nc, int ngrow) {
+    auto d = dst.arr();
+    auto s = src.const_array_impl();
+    const Box b = dst.valid.grow(IntVect(ngrow, ngrow));
+    for (int n = 0; n < nc; ++n) {
+      for (int j = b.lo[1]; j <= b.hi[1]; ++j) {
+        for (int i = b.lo[0]; i <= b.hi[0]; ++i) { d(i, j, 0, dcomp + n) = s(i, j, 0, scomp + n); }
+      }
+    }
+  }
+};
+
+class MFIter {
+ public:
+  const MultiFab* mf;
+  bool valid_ = true;
+  explicit MFIter(const MultiFab& m, bool = false) : mf(&m) {}
+  bool isValid() const noexcept { return valid_; }
+  void operator++() { valid_ = false; }
+  Box validbox() const { return mf->valid; }
+  Box growntilebox(const IntVect& g) const { return mf->valid.grow(g); }
+  int LocalIndex() const { return 0; }
+};
+
+template <class F>
+inline void ParallelFor(const Box& b, F&& f) {
+  for (int j = b.lo[1]; j <= b.hi[1]; ++j) {
+    for (int i = b.lo[0]; i <= b.hi[0]; ++i) { f(i, j, 0); }
+  }
+}
+template <class F>
+inline void ParallelFor(const Box& b, int ncomp, F&& f) {
+  for (int n = 0; n < ncomp; ++n) {
+    for (int j = b.lo[1]; j <= b.hi[1]; ++j) {
+      for (int i = b.lo[0]; i <= b.hi[0]; ++i) { f(i, j, 0, n); }
+    }
+  }
+}
+
+struct ReduceOpSum {
+  template <class T> void local_update(T& d, const T& s) const noexcept { d += s; }
+  template <class T> void init(T& t) const noexcept { t = 0; }
+};
+struct ReduceOpMin {
+  template <class T> void local_update(T& d, const T& s) const noexcept { d = amrex::min(d, s); }
+  template <class T> void init(T& t) const noexcept { t = std::numeric_limits<T>::max(); }
+};
+struct ReduceOpMax {
+  template <class T> void local_update(T& d, const T& s) const noexcept { d = amrex::max(d, s); }
+  template <class T> void init(T& t) const noexcept { t = std::numeric_limits<T>::lowest(); }
+};
+
+template <class... Ps>
+struct ReduceOps {
+  template <class Tuple, std::size_t... I>
+  static void init_all(Tuple& t, std::index_sequence<I...>) { (Ps{}.init(std::get<I>(t)), ...); }
+  template <class Tuple, std::size_t... I>
+  static void update_all(Tuple& d, const Tuple& s, std::index_sequence<I...>) {
+    (Ps{}.local_update(std::get<I>(d), std::get<I>(s)), ...);
+  }
+  template <class D, class F>
+  void eval(const Box& box, D& data, F&& f) {
+    typename D::Type rr;
+    init_all(rr, std::index_sequence_for<Ps...>{});
+    for (int j = box.lo[1]; j <= box.hi[1]; ++j) {
+      for (int i = box.lo[0]; i <= box.hi[0]; ++i) {
+        const typename D::Type v = f(i, j, 0);
+        update_all(rr, v, std::index_sequence_for<Ps...>{});
+      }
+    }
+    update_all(data.r, rr, std::index_sequence_for<Ps...>{});
+  }
+};
+
+template <class... Ts>
+struct ReduceData {
+  using Type = std::tuple<Ts...>;
+  Type r;
+  template <class... Ps>
+  explicit ReduceData(ReduceOps<Ps...>&) { ReduceOps<Ps...>::init_all(r, std::index_sequence_for<Ps...>{}); }
+  Type value() const { return r; }
+};
+
+template <std::size_t I, class T>
+inline decltype(auto) get(T&& t) { return std::get<I>(std::forward<T>(t)); }
+
+namespace ParallelDescriptor {
+inline void ReduceRealSum(Real&) {}
+inline void ReduceRealMin(Real&) {}
+inline void ReduceRealMax(Real&) {}
+inline void ReduceIntSum(int&) {}
+inline void ReduceLongSum(Long&) {}
+inline int NProcs() { return 1; }
+inline bool IOProcessor() { return true; }
+}  // namespace ParallelDescriptor
+
+namespace Gpu {
+inline void streamSynchronize() {}
+}  // namespace Gpu
+
+// ParmParse backed by a process-global key -> values table that the oracle
+// fills from "key=value" lines, as AMReX does from argv.
+inline std::map<std::string, std::vector<std::string>>& parmparse_table() {
+  static std::map<std::string, std::vector<std::string>> t;
+  return t;
+}
+class ParmParse {
+ public:
+  std::string prefix;
+  explicit ParmParse(const std::string& p = "") : prefix(p) {}
+  std::string key(const std::string& n) const { return prefix.empty() ? n : prefix + "." + n; }
+  const std::vector<std::string>* find(const std::string& n) const {
+    auto& t = parmparse_table();
+    auto it = t.find(key(n));
+    return it == t.end() ? nullptr : &it->second;
+  }
+  static bool parse_one(const std::string& s, int& out) {
+    char* end = nullptr;
+    const long v = std::strtol(s.c_str(), &end, 10);
+    if (end == s.c_str()) { Abort("ParmParse: cannot parse '" + s + "' as int"); }
+    out = static_cast<int>(v);
+    return true;
+  }
+  static bool parse_one(const std::string& s, double& out) {
+    char* end = nullptr;
+    const double v = std::strtod(s.c_str(), &end);
+    if (end == s.c_str()) { Abort("ParmParse: cannot parse '" + s + "' as real"); }
+    out = v;
+    return true;
+  }
+  static bool parse_one(const std::string& s, std::string& out) { out = s; return true; }
+  template <class T>
+  bool query(const std::string& n, T& out) const {
+    const auto* v = find(n);
+    if (v == nullptr || v->empty()) { return false; }
+    return parse_one((*v)[0], out);
+  }
+  int countval(const std::string& n) const {
+    const auto* v = find(n);
+    return v == nullptr ? 0 : static_cast<int>(v->size());
+  }
+  template <class T>
+  bool queryarr(const std::string& n, std::vector<T>& out, int start, int num) const {
+    const auto* v = find(n);
+    if (v == nullptr) { return false; }
+    for (int k = 0; k < num && start + k < static_cast<int>(v->size()); ++k) {
+      parse_one((*v)[start + k], out[k]);
+    }
+    return true;
+  }
+};
+
+}  // namespace amrex
