@@ -1,0 +1,187 @@
+"""Python mirror of the reference's hot-path interface, on the CUDA library.
+
+The reference's calls (amrex/apps/euler_compare/src/euler_compare/, all
+inside one translation unit) and their counterparts here:
+
+    euler_fv_one_step(state, geom, cfg, dt, time)         -> euler_fv_one_step(ctx, dt, time)
+        numerics/explicit_update.hpp:58-102
+    compute_euler_dt(state, geom, cfg, time)               -> compute_euler_dt(ctx, time)
+        numerics/diagnostic_metrics_timestep.hpp:227-260
+    compute_imex_dt(state, geom, cfg, time, diag)          -> compute_imex_dt(ctx, time)
+        numerics/diagnostic_metrics_timestep.hpp:272-326
+    compute_diagnostics(state, cfg)                        -> compute_diagnostics(ctx)
+        numerics/diagnostic_metrics_timestep.hpp:18-47
+    compute_admissibility_diagnostics(state, cfg)          -> compute_admissibility_diagnostics(ctx)
+        numerics/diagnostic_metrics_timestep.hpp:49-111
+    fill_problem_ghosts(state, geom, cfg, time)            -> fill_problem_ghosts(ctx, time)
+        problems/boundary_conditions.hpp:202-219
+    euler_imex_bdltv20_o1_source_map_picard_one_step(...)  -> euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, dt)
+        imex/imex_source_map_step.hpp:300-616
+
+The MultiFab becomes a Context holding the device state; numpy arrays of
+shape (4, ny, nx) (components rho, mx, my, E) move it in and out.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import EcgError, check, load
+from .config import RunSettings, read_config
+
+
+def gpu_options(arith="fast", imex_precision="fp64", device=0, tile_y=0, stream=None, **kw):
+    lib = load()
+    o = abi.GpuOptions()
+    lib.ecg_default_gpu_options(C.byref(o))
+    o.device = device
+    o.arith = abi.ARITH_EXACT if arith == "exact" else abi.ARITH_FAST
+    o.imex_precision = abi.IMEX_MIXED if imex_precision == "mixed" else abi.IMEX_FP64
+    o.tile_y = tile_y
+    o.stream = stream
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Context:
+    """One device-resident state (the MultiFab of the reference) and its
+    configuration; owns all device buffers."""
+
+    def __init__(self, cfg, **gpu):
+        lib = load()
+        if isinstance(cfg, RunSettings):
+            cfg = cfg.cfg
+        elif not isinstance(cfg, abi.RunConfig):
+            cfg = read_config(cfg).cfg
+        self.cfg = cfg.copy()
+        self.opt = gpu_options(**gpu)
+        h = C.c_void_p()
+        check(lib.ecg_create(C.byref(h), C.byref(self.cfg), C.byref(self.opt)), "ecg_create")
+        self._h = h
+        self.nx, self.ny = self.cfg.n_cell[0], self.cfg.n_cell[1]
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().ecg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- state exchange (Array4 description of a numpy array) ----
+    def upload(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.shape != (4, self.ny, self.nx):
+            raise ValueError(f"state shape {u.shape} != (4, {self.ny}, {self.nx})")
+        check(load().ecg_upload_state(self._h, u.ctypes.data, 0, 0, self.nx, self.nx * self.ny), "upload", self._h)
+
+    def download(self, out=None):
+        if out is None:
+            out = np.empty((4, self.ny, self.nx), dtype=np.float64)
+        check(load().ecg_download_state(self._h, out.ctypes.data, 0, 0, self.nx, self.nx * self.ny), "download",
+              self._h)
+        return out
+
+    def upload_device(self, ptr, lo=(0, 0), jstride=None, nstride=None):
+        jstride = self.nx if jstride is None else jstride
+        nstride = jstride * self.ny if nstride is None else nstride
+        check(load().ecg_upload_state_device(self._h, ptr, lo[0], lo[1], jstride, nstride), "upload_device", self._h)
+
+    def download_device(self, ptr, lo=(0, 0), jstride=None, nstride=None):
+        jstride = self.nx if jstride is None else jstride
+        nstride = jstride * self.ny if nstride is None else nstride
+        check(load().ecg_download_state_device(self._h, ptr, lo[0], lo[1], jstride, nstride), "download_device",
+              self._h)
+
+    def synchronize(self):
+        check(load().ecg_synchronize(self._h), "synchronize", self._h)
+
+
+def euler_fv_one_step(ctx, dt, time=0.0):
+    """One explicit step; returns the HLLC degenerate-star count."""
+    n = C.c_int32()
+    check(load().ecg_euler_fv_one_step(ctx.handle, dt, time, C.byref(n)), "euler_fv_one_step", ctx.handle)
+    return n.value
+
+
+def compute_euler_dt(ctx, time=0.0):
+    dt = C.c_double()
+    check(load().ecg_compute_euler_dt(ctx.handle, time, C.byref(dt)), "compute_euler_dt", ctx.handle)
+    return dt.value
+
+
+def compute_imex_dt(ctx, time=0.0):
+    dt = C.c_double()
+    d = abi.ImexTimestepDiag()
+    check(load().ecg_compute_imex_dt(ctx.handle, time, C.byref(dt), C.byref(d)), "compute_imex_dt", ctx.handle)
+    return dt.value, d
+
+
+def compute_diagnostics(ctx):
+    d = abi.Diagnostics()
+    check(load().ecg_compute_diagnostics(ctx.handle, C.byref(d)), "compute_diagnostics", ctx.handle)
+    return d
+
+
+def compute_admissibility_diagnostics(ctx):
+    d = abi.Admissibility()
+    check(load().ecg_compute_admissibility_diagnostics(ctx.handle, C.byref(d)), "compute_admissibility_diagnostics",
+          ctx.handle)
+    return d
+
+
+def fill_problem_ghosts(ctx, time=0.0):
+    """The ghosted box (4, ny+4, nx+4) as fill_problem_ghosts leaves it."""
+    g = np.empty((4, ctx.ny + 4, ctx.nx + 4), dtype=np.float64)
+    check(load().ecg_fill_problem_ghosts(ctx.handle, time, g.ctypes.data), "fill_problem_ghosts", ctx.handle)
+    return g
+
+
+def euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, dt):
+    """The IMEX T1/S2 step; returns the diagnostics record.  The state is
+    updated only when the solve converged (as in the reference)."""
+    d = abi.ImexDiag()
+    check(load().ecg_imex_step(ctx.handle, dt, C.byref(d)), "imex step", ctx.handle)
+    return d
+
+
+def solver_status_str(code):
+    return load().ecg_solver_status_str(code).decode()
+
+
+def run(ctx, max_step, stop_time):
+    """The driver's time loop on the device; returns a RunResult."""
+    r = abi.RunResult()
+    check(load().ecg_run(ctx.handle, max_step, stop_time, C.byref(r)), "run", ctx.handle)
+    return r
+
+
+__all__ = [
+    "Context",
+    "EcgError",
+    "compute_admissibility_diagnostics",
+    "compute_diagnostics",
+    "compute_euler_dt",
+    "compute_imex_dt",
+    "euler_fv_one_step",
+    "euler_imex_bdltv20_o1_source_map_picard_one_step",
+    "fill_problem_ghosts",
+    "gpu_options",
+    "read_config",
+    "run",
+    "solver_status_str",
+]

@@ -1,0 +1,76 @@
+// The context behind the opaque ecg_ctx handle of include/ecg.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "ecg.h"
+#include "ecg_internal.h"
+
+struct EcgImexState;  // imex.cu
+
+struct ecg_ctx {
+  static constexpr int kChunk = 32;  // explicit steps per captured graph
+
+  ecg_run_config cfg{};
+  ecg_gpu_options opt{};
+  int device = -1;
+  int num_sms = 0;
+  const EcgStencilOps* ops = nullptr;
+  EcgGrid grid{};
+  int tile_y = 16;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  double* d_state[2] = {nullptr, nullptr};  // double buffer, 4 planes each
+  int cur = 0;
+  bool uploaded = false;
+  double* d_ring = nullptr;                 // ghosted box for exact-state Dirichlet fills
+
+  EcgStepStats* d_stats = nullptr;
+  EcgStepStats* h_stats = nullptr;          // pinned
+  int stats_cap = 0;
+  EcgStateStats* d_state_stats = nullptr;
+  EcgStateStats* h_state_stats = nullptr;   // pinned
+  bool state_stats_valid = false;
+
+  // compute_euler_dt / compute_diagnostics of the current state, reduced by
+  // the fused epilogue of the last explicit step
+  bool fused_valid = false;    // fused_* hold the reductions of the current state
+  bool fused_pending = false;  // they are still in d_stats[1] on the device
+  double fused_max_rate = 0.0, fused_rho_min = 0.0, fused_p_min = 0.0;
+  int fused_nonfinite = 0, fused_degenerate = 0;
+
+  struct Graph {
+    int cur = 0;
+    int max_step = 0;
+    double stop_time = 0.0;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<Graph> graphs;
+
+  EcgImexState* imex = nullptr;
+  std::string err;
+
+  const double* cur_state() const { return d_state[cur]; }
+  double* cur_state_mut() { return d_state[cur]; }
+  double* next_state() { return d_state[cur ^ 1]; }
+  void invalidate() { fused_valid = false; fused_pending = false; state_stats_valid = false; }
+  ~ecg_ctx();
+};
+
+namespace ecgi {
+bool cuda_ok(ecg_ctx* c, cudaError_t e, const char* what);
+double okey_to_double(unsigned long long k);
+EcgFvParams fv_params(ecg_ctx* c, bool imex_policy);
+EcgProblem problem_of(ecg_ctx* c, bool imex_policy);
+bool is_bubble(const ecg_run_config& c);
+bool reduce_state(ecg_ctx* c);
+bool fetch_fused(ecg_ctx* c);
+}  // namespace ecgi
+
+// imex.cu
+void imex_free(ecg_ctx* c);
+ecg_status imex_run(ecg_ctx* c, int32_t max_step, double stop_time, ecg_run_result* out);

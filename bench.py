@@ -1,0 +1,392 @@
+"""Throughput benchmark of the euler_compare hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the configuration the headline metric is quoted on): explicit O2
+HLLC, FP64, on the 2560x640 shock-density-bubble grid (domain [0,2]x[0,0.5],
+reflecting bottom wall, post-shock inflow, outflow right/top; the reference's
+own problem definition), initial state from its initializer.  One step = one
+pass of the hot path over the grid: the fused kernel computes dt from the
+previous step's CFL reduction, reconstructs (MUSCL, minmod), evaluates every
+HLLC face flux, updates the state and reduces the next CFL rate and the
+admissibility diagnostics.
+
+value: cell-updates/s with the state resident in HBM (CUDA events around each
+step on the launching stream; L2 flushed before every timed step by writing a
+256 MiB buffer, since the 52 MB state would otherwise stay in the 126 MB L2).
+e2e: the same metric through the C ABI with HOST buffers: each step uploads the
+caller's state from pinned host memory (ecg_upload_state), steps, and
+downloads it (ecg_download_state), as a drop-in for a host-resident MultiFab
+does.
+
+--impl reference: the reference's own CPU code (oracle/_ref: the reference
+headers built with g++ against a single-box AMReX shim) on
+the same workload, on this machine's host cores (rows split over all host
+threads); one step = the driver's loop
+body compute_euler_dt -> euler_fv_one_step -> compute_diagnostics.
+
+Multi-GPU: the single 2560x640 solve does not shard without a halo exchange,
+so N GPUs run N independent replicas (weak scaling); value is the sum over
+ranks of cells / (max over ranks of the timed region).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY = 2560, 640
+METRIC = "cell-updates/s at 2560x640 FP64 (%HBM); IMEX mixed vs FP64 time at equal L1"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL = 64  # read 4 FP64 conserved values, write 4
+WORKLOAD_KV = {
+    "euler.problem": "shock_density_bubble_2d",
+    "amr.n_cell": f"{NX} {NY}",
+    "euler.method": "explicit",
+    "euler.riemann": "hllc",
+    "euler.spatial_order": 2,
+    "euler.slope_limiter": "minmod",
+    "euler.cfl": 0.45,
+    "stop_time": 1.0,
+}
+CONFIG = {
+    "workload": "shock_density_bubble_2d 2560x640, explicit O2 MUSCL-minmod HLLC, FP64, CFL 0.45",
+    "grid": [NX, NY],
+    "domain": [[0.0, 2.0], [0.0, 0.5]],
+    "riemann": "hllc",
+    "l2": "flushed before every timed step (256 MiB write)",
+    "parallelism": "replicas",
+}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "fv_step_hllc_bubble_2560x640.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(dist, x, device=None):
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, x, device=None):
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU legs (the oracle is a checker/baseline only)
+
+
+def cpu_reference_step_rate(steps, threads=None, grid=(NX, NY)):
+    """The reference's CPU code on the workload: cell-updates/s over `steps`
+    driver-loop bodies on the full grid.  Returns (value, kind, cores, sample)."""
+    from tests.oracle import REF_SO, Oracle, RefOracle
+
+    if threads:
+        os.environ["ECG_REF_THREADS"] = str(threads)
+    kv = dict(WORKLOAD_KV, **{"amr.n_cell": f"{grid[0]} {grid[1]}"})
+    if os.path.exists(REF_SO):
+        r = RefOracle()
+        r.configure(kv)
+        u = r.initialize()
+        t = 0.0
+        dt = r.euler_dt(u, t)
+        r.step(u, dt, t)  # warm
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            dt = r.euler_dt(u, t)
+            u, _ = r.step(u, dt, t)
+            r.diagnostics(u)
+            t += dt
+        el = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        from amrex_euler_allmach_explicit_imex_b200.config import read_config
+
+        o = Oracle()
+        cfg = read_config(kv).cfg
+        u = o.initialize(cfg)
+        t = 0.0
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            dt = o.euler_dt(cfg, u, t)
+            u, _ = o.step(cfg, u, dt, t)
+            o.diagnostics(cfg, u)
+            t += dt
+        el = time.perf_counter() - t0
+        kind = "port"
+    cores = int(os.environ.get("ECG_REF_THREADS", "1")) if kind == "reference" else 1
+    value = grid[0] * grid[1] * steps / el
+    sample = f"{steps} driver-loop steps (dt, euler_fv_one_step, diagnostics) on the full {grid[0]}x{grid[1]} grid"
+    return value, kind, cores, sample
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    steps = max(1, args.steps)
+    from tests.oracle import REF_SO
+
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built on this machine"}))
+        return 0
+    os.environ["ECG_REF_THREADS"] = str(threads)
+    # warmup
+    cpu_reference_step_rate(max(1, min(args.warmup, 2)), threads)
+    value, kind, cores, sample = cpu_reference_step_rate(steps, threads)
+    ms = NX * NY / value * 1e3
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the reference's own shock-density-bubble initializer)", "config": CONFIG,
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+
+
+def run_ours(args):
+    import torch
+
+    from amrex_euler_allmach_explicit_imex_b200 import _lib, api
+    from amrex_euler_allmach_explicit_imex_b200.config import read_config
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(world, "nccl")
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+
+    cfg = read_config(WORKLOAD_KV).cfg
+    stream = torch.cuda.Stream(device=dev)
+    from tests.oracle import Oracle
+
+    # initial state from the reference problem initializer (restated in the
+    # oracle; the product does not depend on it)
+    u0 = Oracle().initialize(cfg)
+    ctx = api.Context(cfg, arith="fast", device=local, stream=stream.cuda_stream)
+    ctx.upload(u0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    cells = NX * NY
+
+    def one_step(t):
+        dt = api.compute_euler_dt(ctx, t)
+        api.euler_fv_one_step(ctx, dt, t)
+        return t + dt
+
+    # ---- device-resident throughput -----------------------------------------------------
+    t = 0.0
+    for _ in range(args.warmup):
+        t = one_step(t)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    dts = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(dev)
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            dt = api.compute_euler_dt(ctx, t)  # host read of the previous step's fused CFL reduction
+            ev[k][0].record(stream)
+            api.euler_fv_one_step(ctx, dt, t)
+            ev[k][1].record(stream)
+            dts.append(dt)
+            t += dt
+        torch.cuda.synchronize(dev)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if dist is not None:
+        dist.barrier()
+    total_ms = max_over_ranks(dist, total_ms, dev)
+    value = sum_over_ranks(dist, cells * args.steps, dev) / (total_ms * 1e-3)
+    kern_s = (total_ms / args.steps) * 1e-3
+    achieved = BYTES_PER_CELL * cells / kern_s / 1e9
+    peak, peak_kind = peaks()
+    d = api.compute_diagnostics(ctx)
+    ok = d.nonfinite_count == 0 and d.rho_min > 0 and d.pressure_min > 0
+
+    # ---- end to end through the C ABI with host buffers ----------------------------------
+    host_in = torch.from_numpy(u0).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    hp_in, hp_out = host_in.data_ptr(), host_out.data_ptr()
+    e2e_k = max(3, min(args.steps, 10))
+    te = 0.0
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(e2e_k):
+        _lib.check(lib.ecg_upload_state(ctx.handle, hp_in, 0, 0, NX, NX * NY), "upload")
+        dt = api.compute_euler_dt(ctx, te)
+        api.euler_fv_one_step(ctx, dt, te)
+        _lib.check(lib.ecg_download_state(ctx.handle, hp_out, 0, 0, NX, NX * NY), "download")
+        te += dt
+    e_end.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(dist, e_start.elapsed_time(e_end), dev)
+    e2e_value = sum_over_ranks(dist, cells * e2e_k, dev) / (e2e_ms * 1e-3)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, kind, cores, sample = cpu_reference_step_rate(args.cpu_steps, os.cpu_count())
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        traffic = profile_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the reference's own shock-density-bubble initializer)", "config": CONFIG,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "note": "algorithmic bytes = 64 B x 1,638,400 cells per launch; event time of the fused step kernel"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * cells,
+                    "d2h_bytes_per_step": 32 * cells},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+            "state_ok": bool(ok),
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -31,6 +31,8 @@
 #include <utility>
 #include <vector>
 
+#include <thread>
+
 #define AMREX_SPACEDIM 2
 #define AMREX_GPU_HOST_DEVICE
 #define AMREX_GPU_DEVICE
@@ -237,18 +239,45 @@ class MFIter {
   int LocalIndex() const { return 0; }
 };
 
+// Row-parallel execution for the timed CPU baseline: ECG_REF_THREADS host
+// threads share the rows of a box (default 1 = AMReX's serial CPU order).
+// Every cell is written by exactly one iteration, so results do not depend on
+// the thread count.
+inline int shim_threads() {
+  const char* e = std::getenv("ECG_REF_THREADS");
+  const int v = e ? std::atoi(e) : 1;
+  return v < 1 ? 1 : v;
+}
+template <class Body>
+inline void parallel_rows(int lo, int hi, Body&& body) {
+  const int nt = shim_threads();
+  const int n = hi - lo + 1;
+  if (nt <= 1 || n < 2 * nt) {
+    for (int j = lo; j <= hi; ++j) body(0, j);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve(static_cast<std::size_t>(nt));
+  for (int t = 0; t < nt; ++t) {
+    const int a = lo + static_cast<int>(static_cast<long long>(t) * n / nt);
+    const int b = lo + static_cast<int>(static_cast<long long>(t + 1) * n / nt);
+    th.emplace_back([&body, a, b, t] { for (int j = a; j < b; ++j) body(t, j); });
+  }
+  for (auto& x : th) x.join();
+}
+
 template <class F>
 inline void ParallelFor(const Box& b, F&& f) {
-  for (int j = b.lo[1]; j <= b.hi[1]; ++j) {
+  parallel_rows(b.lo[1], b.hi[1], [&](int, int j) {
     for (int i = b.lo[0]; i <= b.hi[0]; ++i) { f(i, j, 0); }
-  }
+  });
 }
 template <class F>
 inline void ParallelFor(const Box& b, int ncomp, F&& f) {
   for (int n = 0; n < ncomp; ++n) {
-    for (int j = b.lo[1]; j <= b.hi[1]; ++j) {
+    parallel_rows(b.lo[1], b.hi[1], [&](int, int j) {
       for (int i = b.lo[0]; i <= b.hi[0]; ++i) { f(i, j, 0, n); }
-    }
+    });
   }
 }
 
@@ -273,16 +302,23 @@ struct ReduceOps {
   static void update_all(Tuple& d, const Tuple& s, std::index_sequence<I...>) {
     (Ps{}.local_update(std::get<I>(d), std::get<I>(s)), ...);
   }
+  // Serial: cells in AMReX's CPU order (i fastest).  Threaded: partials over
+  // contiguous row blocks, combined in block order (min, max and integer sums
+  // are unchanged; floating-point sums may round differently).
   template <class D, class F>
   void eval(const Box& box, D& data, F&& f) {
     typename D::Type rr;
     init_all(rr, std::index_sequence_for<Ps...>{});
-    for (int j = box.lo[1]; j <= box.hi[1]; ++j) {
+    const int nt = shim_threads();
+    std::vector<typename D::Type> part(static_cast<std::size_t>(nt));
+    for (auto& p : part) init_all(p, std::index_sequence_for<Ps...>{});
+    parallel_rows(box.lo[1], box.hi[1], [&](int t, int j) {
       for (int i = box.lo[0]; i <= box.hi[0]; ++i) {
         const typename D::Type v = f(i, j, 0);
-        update_all(rr, v, std::index_sequence_for<Ps...>{});
+        update_all(part[static_cast<std::size_t>(t)], v, std::index_sequence_for<Ps...>{});
       }
-    }
+    });
+    for (const auto& p : part) update_all(rr, p, std::index_sequence_for<Ps...>{});
     update_all(data.r, rr, std::index_sequence_for<Ps...>{});
   }
 };

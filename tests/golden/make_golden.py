@@ -1,0 +1,198 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Run where the reference sources are present (it builds and loads
+oracle/_ref/libecg_ref.so, the reference's own headers compiled against the
+single-box AMReX shim):
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Every number in the fixtures is the reference's output on seeded inputs.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from amrex_euler_allmach_explicit_imex_b200 import abi  # noqa: E402
+from tests.oracle import RefOracle  # noqa: E402
+
+RIEMANNS = ["hllc", "rusanov", "lowmach_hllc", "xie_am_hllc_p"]
+LIMITERS = ["minmod", "mc", "vanleer"]
+BCS = ["periodic", "outflow", "mixed", "bubble", "toro_exact", "gresho_exact", "quadrant_exact", "blob_exact"]
+
+
+def kv_text(kv):
+    return "\n".join(f"{k}={v}" for k, v in kv.items())
+
+
+def rand_state(rng, nx, ny, gamma=1.4, lowmach=False):
+    rho = rng.uniform(0.2, 2.0, (ny, nx))
+    u = rng.uniform(-1, 1, (ny, nx))
+    v = rng.uniform(-1, 1, (ny, nx))
+    p = rng.uniform(0.2, 2.0, (ny, nx))
+    if lowmach:
+        u *= 0.01
+        v *= 0.01
+        p = 1.0 / (1.4 * 1e-4) + rng.uniform(0, 1, (ny, nx))
+    E = p / (gamma - 1) + 0.5 * rho * (u * u + v * v)
+    return np.stack([rho, rho * u, rho * v, E])
+
+
+def explicit_cases(r):
+    rng = np.random.default_rng(20261203)
+    out = {}
+    idx = 0
+    for riem in RIEMANNS:
+        for lim in LIMITERS:
+            for bc in BCS:
+                kv = {"amr.n_cell": "9 7", "euler.riemann": riem, "euler.slope_limiter": lim,
+                      "euler.spatial_order": 2, "euler.method": "explicit"}
+                if bc == "periodic":
+                    kv["geometry.is_periodic"] = "1 1"
+                elif bc == "outflow":
+                    kv["geometry.is_periodic"] = "0 0"
+                elif bc == "mixed":
+                    kv["geometry.is_periodic"] = "0 1"
+                elif bc == "bubble":
+                    if riem not in ("hllc", "xie_am_hllc_p"):
+                        continue
+                    kv.update({"euler.problem": "shock_density_bubble_2d", "amr.n_cell": "16 5"})
+                elif bc == "toro_exact":
+                    kv.update({"euler.problem": "toro1", "euler.field_boundary": "exact_dirichlet",
+                               "geometry.is_periodic": "0 1", "prob.test": "1"})
+                elif bc == "gresho_exact":
+                    kv.update({"euler.problem": "gresho_vortex", "euler.field_boundary": "exact_dirichlet",
+                               "geometry.is_periodic": "0 0", "euler.vortex_center": "0.5 0.5"})
+                elif bc == "quadrant_exact":
+                    kv.update({"euler.problem": "riemann_quadrant", "euler.field_boundary": "exact_dirichlet",
+                               "geometry.is_periodic": "1 0"})
+                elif bc == "blob_exact":
+                    kv.update({"euler.problem": "advection_blob", "euler.field_boundary": "exact_dirichlet",
+                               "geometry.is_periodic": "0 1"})
+                if lim != "minmod" and bc in ("quadrant_exact", "blob_exact", "mixed"):
+                    continue
+                cfg = r.configure(kv)
+                nx, ny = cfg.n_cell[0], cfg.n_cell[1]
+                u0 = rand_state(rng, nx, ny, lowmach=(riem == "xie_am_hllc_p" and lim == "mc"))
+                t = 0.013
+                dt = 0.3 * r.euler_dt(u0, t)
+                u1, deg = r.step(u0, dt, t)
+                d = r.diagnostics(u1)
+                a = r.admissibility(u1)
+                tdt, td = r.imex_dt(u1, t)
+                key = f"c{idx:03d}"
+                out[key + "_kv"] = np.array(kv_text(kv))
+                out[key + "_u0"] = u0
+                out[key + "_dt"] = np.array(dt)
+                out[key + "_t"] = np.array(t)
+                out[key + "_u1"] = u1
+                out[key + "_deg"] = np.array(deg)
+                out[key + "_ghost"] = r.fill_ghosts(u0, t)
+                out[key + "_edt"] = np.array(r.euler_dt(u1, t))
+                out[key + "_diag"] = np.array([d.rho_min, d.pressure_min, d.nonfinite_count])
+                out[key + "_adm"] = np.array([a.rho_min, a.pressure_min, a.internal_energy_min, a.nonfinite_count,
+                                              a.density_failure_count, a.pressure_failure_count,
+                                              a.internal_energy_failure_count])
+                out[key + "_imexdt"] = np.array([tdt, td.material_rate_max, td.acoustic_rate_max])
+                idx += 1
+    out["count"] = np.array(idx)
+    return out
+
+
+SOD = {"amr.n_cell": "400 4", "amr.max_grid_size": 400, "geometry.prob_lo": "0 0", "geometry.prob_hi": "1 0.01",
+       "geometry.is_periodic": "0 1", "euler.problem": "toro1", "prob.test": 1, "prob.x0": 0.5,
+       "euler.method": "explicit", "euler.spatial_order": 2, "euler.riemann": "hllc",
+       "euler.slope_limiter": "minmod", "euler.cfl": 0.5, "stop_time": 0.2, "max_step": 100000,
+       "euler.field_boundary": "outflow"}
+
+
+def sod_case(r):
+    r.configure(SOD)
+    u = r.initialize()
+    out = {"kv": np.array(kv_text(SOD)), "u0": u.copy()}
+    t, step, dts, degs = 0.0, 0, [], []
+    while step < 100000 and t < 0.2 - 1e-14:
+        dt = r.euler_dt(u, t)
+        u, deg = r.step(u, dt, t)
+        dts.append(dt)
+        degs.append(deg)
+        t += dt
+        step += 1
+        if step == 1:
+            out["u1"] = u.copy()
+    nx = 400
+    xs = (np.arange(nx) + 0.5) / nx
+    ex = np.array([r.exact_riemann(x, t, [1.0, 0, 0, 1.0], [0.125, 0, 0, 0.1], 1.4, 0.5)[0] for x in xs])
+    out.update(steps=np.array(step), time=np.array(t), dts=np.array(dts), degs=np.array(degs), u_final=u,
+               exact_rho=ex, l1_rho=np.array(np.abs(u[0] - ex[None, :]).mean()))
+    return out
+
+
+IMEX_BASE = {"euler.method": "imex", "euler.spatial_order": 2, "euler.imex_acoustic_startup": 0,
+             "euler.imex_picard_iterations": 4, "euler.imex_solver_tol": "1e-10", "euler.imex_solver_max_iter": 200,
+             "euler.imex_cfl": 0.4}
+IMEX_CASES = {
+    "gresho_m0p1": dict(IMEX_BASE, **{"amr.n_cell": "24 24", "euler.problem": "gresho_vortex",
+                                       "euler.vortex_center": "0.5 0.5", "euler.mach": 0.1,
+                                       "euler.pressure": repr(1 / (1.4 * 0.01)), "geometry.is_periodic": "1 1"}),
+    "gresho_m0p01": dict(IMEX_BASE, **{"amr.n_cell": "24 24", "euler.problem": "gresho_vortex",
+                                        "euler.vortex_center": "0.5 0.5", "euler.mach": 0.01,
+                                        "euler.pressure": repr(1 / (1.4 * 1e-4)), "geometry.is_periodic": "1 1"}),
+    "bubble": dict(IMEX_BASE, **{"amr.n_cell": "32 8", "euler.problem": "shock_density_bubble_2d",
+                                  "euler.imex_cfl": 0.45}),
+    "sod_reflect": dict(IMEX_BASE, **{"amr.n_cell": "32 4", "euler.problem": "toro1", "geometry.is_periodic": "0 0",
+                                       "geometry.prob_hi": "1 0.125"}),
+}
+
+
+def imex_cases(r):
+    out = {}
+    for name, kv in IMEX_CASES.items():
+        r.configure(kv)
+        u0 = r.initialize()
+        dt, _ = r.imex_dt(u0)
+        u1, d = r.imex_step(u0, dt)
+        out[name + "_kv"] = np.array(kv_text(kv))
+        out[name + "_u0"] = u0
+        out[name + "_dt"] = np.array(dt)
+        out[name + "_u1"] = u1
+        for f in abi.IMEX_DIAG_INT_FIELDS + abi.IMEX_DIAG_REAL_FIELDS:
+            out[name + "_d_" + f] = np.array(getattr(d, f))
+        # pieces of the first Picard iteration on a perturbed state
+        rng = np.random.default_rng(7)
+        up = u0 * (1 + 0.02 * rng.standard_normal(u0.shape))
+        star = r.imex_star(up, dt)
+        p = 0.4 * (up[3] - 0.5 * (up[1] ** 2 + up[2] ** 2) / up[0])
+        k = np.stack([star[1], star[2]]) * (1 + 0.05 * rng.standard_normal((2,) + u0.shape[1:]))
+        rp, col, val, rhs, nf = r.build_system(star, p, k, dt)
+        g = r.gmres_csr(rp, col, val, rhs, p.ravel(), 200, 1e-10)
+        out[name + "_pu"] = up
+        out[name + "_pstar"] = star
+        out[name + "_pp"] = p
+        out[name + "_pk"] = k
+        out[name + "_prp"] = rp
+        out[name + "_pcol"] = col
+        out[name + "_pval"] = val
+        out[name + "_prhs"] = rhs
+        out[name + "_pkcorr"] = r.corrected_momentum(star, p, dt)
+        out[name + "_gx"] = g["x"]
+        out[name + "_giters"] = np.array(g["iterations"])
+    return out
+
+
+def main():
+    r = RefOracle()
+    np.savez_compressed(os.path.join(HERE, "explicit_cases.npz"), **explicit_cases(r))
+    np.savez_compressed(os.path.join(HERE, "sod_400x4.npz"), **sod_case(r))
+    np.savez_compressed(os.path.join(HERE, "imex_cases.npz"), **imex_cases(r))
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()
