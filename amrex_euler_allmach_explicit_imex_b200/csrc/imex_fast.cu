@@ -1,0 +1,8 @@
+// IMEX stencil kernels built with -fmad=true (default arithmetic mode).
+#include <string>
+#define ECG_NS ecg_fast
+#include "imex_kernels.cuh"
+
+const EcgImexOps ecg_imex_fast_ops = {ecg_fast::imex_star,     ecg_fast::imex_faces,    ecg_fast::imex_rhs,
+                                      ecg_fast::imex_p_update, ecg_fast::imex_momentum, ecg_fast::imex_closeout,
+                                      ecg_fast::imex_eq78};

@@ -1,0 +1,109 @@
+// Structures of the IMEX path shared by its translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "ecg_internal.h"
+
+// Index maps and physical-boundary states of the IMEX host grid
+// (imex/imex_source_map_helpers.hpp:70-245).
+struct EcgImexMap {
+  int nx, ny, px, py, bubble, pad;
+  double gamma;
+  double cst[4];    // bubble post-shock conserved state
+  double p_fixed;   // bubble fixed post-shock pressure
+};
+
+// Reductions of the IMEX kernels (min/max as ordered keys, counts, sums).
+struct EcgImexStats {
+  // star + initialisation
+  unsigned long long floor_count;
+  unsigned long long k_nonfinite;
+  unsigned long long trial_rho_min_key;
+  unsigned long long mismatch_before_key;
+  unsigned long long mismatch_before_nonfinite;
+  // pressure system
+  unsigned long long row_nonfinite;
+  unsigned long long nnz;
+  unsigned long long max_row_width;
+  unsigned long long abs_max_key;
+  unsigned long long sym_key;
+  unsigned long long rhs_linf_key;
+  // Picard update
+  unsigned long long delta_linf_key;
+  unsigned long long pmax_key;
+  double delta_l2_sum;
+  // closeout
+  unsigned long long guard, h_nonfinite, flux_nonfinite, final_nonfinite;
+  unsigned long long density_fail, pressure_fail, ie_fail, residual_count;
+  unsigned long long flux_linf_key, density_min_key, solved_p_min_key, solved_p_max_key;
+  unsigned long long eos_p_min_key, eos_p_max_key, ie_min_key, ie_max_key;
+  unsigned long long momentum_corr_key, energy_corr_key, flux_div_key;
+  unsigned long long res_linf_key, res_rel_key, mis_linf_key, mis_rel_key;
+  double res_sum, mis_sum, energy_sum;
+  unsigned long long eq78_count, eq78_key, eq78_scaled_key;
+};
+
+// Function table of one arithmetic build of the IMEX stencil kernels.
+struct EcgImexOps {
+  cudaError_t (*star)(const EcgFvParams& P, const double* u, double dt, double* S, double* p, double* K,
+                      EcgImexStats* st, cudaStream_t s);
+  cudaError_t (*faces)(const EcgImexMap& m, const double* S, const double* p, const double* K, double* fx, double* fy,
+                       unsigned char* fxf, unsigned char* fyf, int mode, cudaStream_t s);
+  cudaError_t (*rhs)(const EcgImexMap& m, const double* S, const double* K, const double* hx, const double* hy,
+                     double dt, double idx, double idy, int matrix_diag, double* rhs, EcgImexStats* st, cudaStream_t s);
+  cudaError_t (*p_update)(long long n, double* p, const double* x, EcgImexStats* st, cudaStream_t s);
+  cudaError_t (*momentum)(const EcgImexMap& m, const double* S, const double* p, double dt, double idx, double idy,
+                          double* K, EcgImexStats* st, cudaStream_t s);
+  cudaError_t (*closeout)(const EcgImexMap& m, const EcgGrid& G, const double* S, const double* p, const double* K,
+                          const double* fx, const double* fy, const unsigned char* fxf, const unsigned char* fyf,
+                          double dt, double* out, EcgImexStats* st, cudaStream_t s);
+  cudaError_t (*eq78)(const EcgImexMap& m, const EcgGrid& G, const double* S, const double* K, EcgImexStats* st,
+                      cudaStream_t s);
+};
+
+extern const EcgImexOps ecg_imex_exact_ops;
+extern const EcgImexOps ecg_imex_fast_ops;
+
+// ---- GMRES (gmres.cu) -------------------------------------------------------------------
+
+// Matrix-free pressure operator of source_map_pressure_row_data
+// (imex_source_map_helpers.hpp:533-543) from the face enthalpies.
+struct EcgPressureOp {
+  int nx, ny, px, py, bubble, pad;
+  double diag0;      // 1 / (gamma - 1)
+  double xc, yc;     // dt^2 / (4 dx^2), dt^2 / (4 dy^2)
+  const double* hx;  // (nx+1) x ny
+  const double* hy;  // nx x (ny+1)
+  const float* hx32; // FP32 copies for the mixed-precision inner solve
+  const float* hy32;
+};
+
+struct EcgGmresResult {
+  int iterations;      // index of the returned iterate
+  int converged;
+  int breakdown;
+  int nonfinite;
+  int timeout;         // a bounded grid barrier gave up
+  int inner_iterations;
+  int refinements;
+  int pad;
+  double residual_linf;
+  double relative_residual_linf;
+};
+
+struct EcgGmresWork;  // gmres.cu
+
+EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int device, bool mixed, std::string* err);
+void gmres_work_destroy(EcgGmresWork* w);
+// Solves A x = b from x0 (device vectors of n doubles) with the reference's
+// semantics (solve_host_sparse_gmres, imex/imex_pressure_helpers.hpp:92-217).
+// mixed: FP32 inner GMRES inside FP64 iterative refinement.
+cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
+                        int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
+                        EcgGmresResult* out, cudaStream_t s);
+// r = A x - b: infinity norm, rhs infinity norm (max(|b|inf, 1)) and nonfinite flag.
+cudaError_t pressure_residual(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x,
+                              double* res_linf, double* rhs_norm, int* nonfinite, cudaStream_t s);

@@ -1,0 +1,819 @@
+// Kernels of the IMEX T1/S2 BDLTV20 source-map step
+// (imex/imex_source_map_step.hpp:300-616 and imex/imex_source_map_helpers.hpp):
+// star update, face enthalpies, pressure-row right-hand side and matrix
+// diagnostics, the matrix-free pressure operator, the Picard refresh and the
+// conservative closeout.  Vectors are compact row-major (row = j*nx + i).
+//
+// Included by imex_exact.cu (-fmad=false) and imex_fast.cu (-fmad=true).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "ecg.h"
+#include "ecg_internal.h"
+#include "imex_internal.h"
+
+namespace ECG_NS {
+
+#include "ecg_device.cuh"
+
+namespace imexk {
+
+constexpr double kInf = __builtin_huge_val();
+constexpr double kLowest = -1.7976931348623157e308;
+constexpr double kMax = 1.7976931348623157e308;
+
+__device__ __forceinline__ int wrapi(int i, int n)
+{
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+__device__ __forceinline__ int clampi(int i, int n) { return i < 0 ? 0 : (i > n - 1 ? n - 1 : i); }
+
+// CoupledHostGrid::map_i / map_j (imex_source_map_helpers.hpp:79-93)
+__device__ __forceinline__ int mi(const EcgImexMap& m, int i) { return m.px ? wrapi(i, m.nx) : clampi(i, m.nx); }
+__device__ __forceinline__ int mj(const EcgImexMap& m, int j) { return m.py ? wrapi(j, m.ny) : clampi(j, m.ny); }
+
+// source_map_index (imex_source_map_helpers.hpp:169-188): wrap or even reflection
+__device__ __forceinline__ int pmap(int k, int n, int per)
+{
+  if (per) return wrapi(k, n);
+  if (k < 0) {
+    const int r = -k - 1;
+    return r < n - 1 ? r : n - 1;
+  }
+  if (k >= n) {
+    const int r = n - (k - n + 1);
+    return r > 0 ? r : 0;
+  }
+  return k;
+}
+__device__ __forceinline__ int prow(const EcgImexMap& m, int i, int j)
+{
+  return pmap(j, m.ny, m.py) * m.nx + pmap(i, m.nx, m.px);
+}
+
+__device__ __forceinline__ Cons star_at(const EcgImexMap& m, const double* __restrict__ S, int i, int j)
+{
+  const long long r = static_cast<long long>(mj(m, j)) * m.nx + mi(m, i);
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  return Cons{S[r], S[r + n], S[r + 2 * n], S[r + 3 * n]};
+}
+
+// source_map_state_at_physical_boundary (imex_source_map_helpers.hpp:98-115)
+__device__ __forceinline__ Cons state_b(const EcgImexMap& m, const double* __restrict__ S, int i, int j)
+{
+  if (m.bubble) {
+    if (!m.px && i < 0) return Cons{m.cst[0], m.cst[1], m.cst[2], m.cst[3]};
+    const int ii = mi(m, i);
+    if (!m.py && j < 0) {
+      Cons c = star_at(m, S, ii, 0);
+      c.my = -c.my;
+      return c;
+    }
+    return star_at(m, S, ii, j);
+  }
+  return star_at(m, S, i, j);
+}
+
+// source_map_pressure_at_physical_boundary (imex_source_map_helpers.hpp:222-245)
+__device__ __forceinline__ double p_b(const EcgImexMap& m, const double* __restrict__ p, int i, int j)
+{
+  if (m.bubble && !m.px && i < 0) return m.p_fixed;
+  return p[prow(m, i, j)];
+}
+
+// source_map_lagged_momentum_at(_physical_boundary) (imex_source_map_helpers.hpp:293-320)
+__device__ __forceinline__ void m_at(const EcgImexMap& m, const double* __restrict__ K, int i, int j, double& m0,
+                                     double& m1)
+{
+  const long long r = static_cast<long long>(mj(m, j)) * m.nx + mi(m, i);
+  m0 = K[r];
+  m1 = K[r + static_cast<long long>(m.nx) * m.ny];
+}
+__device__ __forceinline__ void m_b(const EcgImexMap& m, const double* __restrict__ K, int i, int j, double& m0,
+                                    double& m1)
+{
+  if (m.bubble) {
+    if (!m.px && i < 0) {
+      m0 = m.cst[1];
+      m1 = m.cst[2];
+      return;
+    }
+    const int ii = mi(m, i);
+    if (!m.py && j < 0) {
+      m_at(m, K, ii, 0, m0, m1);
+      m1 = -m1;
+      return;
+    }
+  }
+  m_at(m, K, i, j, m0, m1);
+}
+
+struct FaceOut {
+  double h_hat, flux;
+  int flags;  // bit0 guard, bit1 enthalpy inputs nonfinite, bit2 flux nonfinite
+};
+
+// source_map_face_flux_detail (imex_source_map_helpers.hpp:359-402)
+__device__ __forceinline__ FaceOut face_detail(const EcgImexMap& m, const double* __restrict__ S,
+                                               const double* __restrict__ p, const double* __restrict__ K, int il,
+                                               int jl, int ir, int jr, int axis)
+{
+  const double gm1 = m.gamma - 1.0;
+  const Cons L = state_b(m, S, il, jl), R = state_b(m, S, ir, jr);
+  double ml0, ml1, mr0, mr1;
+  m_b(m, K, il, jl, ml0, ml1);
+  m_b(m, K, ir, jr, mr0, mr1);
+  const double pl = p_b(m, p, il, jl), pr = p_b(m, p, ir, jr);
+  const double hl = m.gamma * pl / (gm1 * L.rho);
+  const double hr = m.gamma * pr / (gm1 * R.rho);
+  const double ql = axis == 0 ? ml0 : ml1;
+  const double qr = axis == 0 ? mr0 : mr1;
+  const double den = ql + qr;
+  const double scale = smax(smax(fabs(ql), fabs(qr)), 1.0);
+  const int guard = fabs(den) <= 1.0e-14 * scale ? 1 : 0;
+  const double h = guard ? 0.5 * (hl + hr) : (hl * ql + hr * qr) / den;
+  const double mh = 0.5 * (ql + qr);
+  FaceOut o;
+  o.h_hat = h;
+  o.flux = h * mh;
+  o.flags = guard | ((!isfinite(hl) || !isfinite(hr) || !isfinite(h) || !isfinite(ql) || !isfinite(qr)) ? 2 : 0) |
+            (isfinite(o.flux) ? 0 : 4);
+  return o;
+}
+
+// ---- block reduction helpers ------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a > b ? a : b; }
+__device__ __forceinline__ unsigned long long umin64(unsigned long long a, unsigned long long b) { return a < b ? a : b; }
+
+template <int NT>
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* sh)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = umax64(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < NT / 32; ++w) v = umax64(v, sh[w]);
+  __syncthreads();
+  return v;
+}
+template <int NT>
+__device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v, unsigned long long* sh)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = umin64(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < NT / 32; ++w) v = umin64(v, sh[w]);
+  __syncthreads();
+  return v;
+}
+template <int NT>
+__device__ __forceinline__ long long block_sum_i64(long long v, long long* sh)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < NT / 32; ++w) v += sh[w];
+  __syncthreads();
+  return v;
+}
+template <int NT>
+__device__ __forceinline__ double block_sum_f64(double v, double* sh)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < NT / 32; ++w) v += sh[w];
+  __syncthreads();
+  return v;
+}
+
+struct Shared {
+  unsigned long long u[32];
+  long long l[32];
+  double d[32];
+};
+
+#define ECG_RED_MAX(field, val)                                              \
+  {                                                                          \
+    const unsigned long long _v = block_max_u64<NT>((val), sh.u);            \
+    if (threadIdx.x == 0) atomicMax(&(field), _v);                           \
+  }
+#define ECG_RED_MIN(field, val)                                              \
+  {                                                                          \
+    const unsigned long long _v = block_min_u64<NT>((val), sh.u);            \
+    if (threadIdx.x == 0) atomicMin(&(field), _v);                           \
+  }
+#define ECG_RED_ADD_I(field, val)                                            \
+  {                                                                          \
+    const long long _v = block_sum_i64<NT>((val), sh.l);                     \
+    if (threadIdx.x == 0 && _v) atomicAdd(&(field), static_cast<unsigned long long>(_v)); \
+  }
+#define ECG_RED_ADD_D(field, val)                                            \
+  {                                                                          \
+    const double _v = block_sum_f64<NT>((val), sh.d);                        \
+    if (threadIdx.x == 0) atomicAdd(&(field), _v);                           \
+  }
+
+// ---- star update -----------------------------------------------------------------
+
+// Conserved-minmod reconstruction of cell c0 to side h (BDLTV20 eq 87-89),
+// reconstruction_fluxes.hpp:26-52.
+__device__ __forceinline__ Prim recon_cmm(const Cons& um, const Cons& u, const Cons& up, double h, double g)
+{
+  const Cons s{minmod(u.rho - um.rho, up.rho - u.rho), minmod(u.mx - um.mx, up.mx - u.mx),
+               minmod(u.my - um.my, up.my - u.my), minmod(u.E - um.E, up.E - u.E)};
+  return to_prim(Cons{u.rho + h * s.rho, u.mx + h * s.mx, u.my + h * s.my, u.E + h * s.E}, g);
+}
+
+// bdltv20_pressure_split_lf_flux with material speed, reconstruction_fluxes.hpp:462-484,504-515
+__device__ __forceinline__ Cons split_lf(const Prim& l, const Prim& r, int axis, double g)
+{
+  const Cons ul = to_cons(l, g), ur = to_cons(r, g);
+  const double lmx = l.rho * l.u, lmy = l.rho * l.v, lk = 0.5 * l.rho * (l.u * l.u + l.v * l.v);
+  const double rmx = r.rho * r.u, rmy = r.rho * r.v, rk = 0.5 * r.rho * (r.u * r.u + r.v * r.v);
+  Cons fl, fr;
+  if (axis == 0) {
+    fl = Cons{lmx, lmx * l.u, lmy * l.u, lk * l.u};
+    fr = Cons{rmx, rmx * r.u, rmy * r.u, rk * r.u};
+  } else {
+    fl = Cons{lmy, lmx * l.v, lmy * l.v, lk * l.v};
+    fr = Cons{rmy, rmx * r.v, rmy * r.v, rk * r.v};
+  }
+  const double sm = smax(fabs(normal_vel(l, axis)), fabs(normal_vel(r, axis)));
+  const double hs = 0.5 * sm;
+  return Cons{0.5 * (fl.rho + fr.rho) - hs * (ur.rho - ul.rho), 0.5 * (fl.mx + fr.mx) - hs * (ur.mx - ul.mx),
+              0.5 * (fl.my + fr.my) - hs * (ur.my - ul.my), 0.5 * (fl.E + fr.E) - hs * (ur.E - ul.E)};
+}
+
+// Ghost-aware conserved state of the old state (IMEX ghost policy).
+__device__ __forceinline__ Cons old_cell(const EcgFvParams& P, const double* __restrict__ u, int i, int j);
+
+// compute_bdltv20_pressure_split_star (imex_source_map_helpers.hpp:2-68) with
+// the step's initialisation fused in: p0 = pressure of U^n
+// (imex_source_map_step.hpp:422-434), K0 = star momentum (:418), the density
+// floor check (:436-451) and the star pressure mismatch (:278-298,453-454).
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_star_kernel(const EcgFvParams P, const double* __restrict__ u,
+                                                       const double dt, double* __restrict__ S, double* __restrict__ p,
+                                                       double* __restrict__ K, EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const int nx = P.g.nx, ny = P.g.ny;
+  const long long n = static_cast<long long>(nx) * ny;
+  const double g = P.gamma, idx = P.g.inv_dx, idy = P.g.inv_dy;
+  long long floor_count = 0, knf = 0;
+  unsigned long long rho_min = okey(kInf), mis = okey(0.0);
+  long long mis_nf = 0;
+  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
+       r += static_cast<long long>(gridDim.x) * NT) {
+    const int i = static_cast<int>(r % nx), j = static_cast<int>(r / nx);
+    const Cons c = old_cell(P, u, i, j);
+    const Cons w = old_cell(P, u, i - 1, j), e = old_cell(P, u, i + 1, j);
+    const Cons s_ = old_cell(P, u, i, j - 1), nn = old_cell(P, u, i, j + 1);
+    const Cons ww = old_cell(P, u, i - 2, j), ee = old_cell(P, u, i + 2, j);
+    const Cons ss = old_cell(P, u, i, j - 2), n2 = old_cell(P, u, i, j + 2);
+    const Cons fxl = split_lf(recon_cmm(ww, w, c, 0.5, g), recon_cmm(w, c, e, -0.5, g), 0, g);
+    const Cons fxr = split_lf(recon_cmm(w, c, e, 0.5, g), recon_cmm(c, e, ee, -0.5, g), 0, g);
+    const Cons fyb = split_lf(recon_cmm(ss, s_, c, 0.5, g), recon_cmm(s_, c, nn, -0.5, g), 1, g);
+    const Cons fyt = split_lf(recon_cmm(s_, c, nn, 0.5, g), recon_cmm(c, nn, n2, -0.5, g), 1, g);
+    const Cons up{c.rho - dt * ((fxr.rho - fxl.rho) * idx + (fyt.rho - fyb.rho) * idy),
+                  c.mx - dt * ((fxr.mx - fxl.mx) * idx + (fyt.mx - fyb.mx) * idy),
+                  c.my - dt * ((fxr.my - fxl.my) * idx + (fyt.my - fyb.my) * idy),
+                  c.E - dt * ((fxr.E - fxl.E) * idx + (fyt.E - fyb.E) * idy)};
+    S[r] = up.rho;
+    S[r + n] = up.mx;
+    S[r + 2 * n] = up.my;
+    S[r + 3 * n] = up.E;
+    K[r] = up.mx;
+    K[r + n] = up.my;
+    const double p0 = to_prim(c, g).p;
+    p[r] = p0;
+    if (!isfinite(up.mx) || !isfinite(up.my)) ++knf;
+    if (!isfinite(up.rho) || up.rho <= 1.0e-14) ++floor_count;
+    if (isfinite(up.rho)) rho_min = umin64(rho_min, okey(up.rho));
+    const double kin = 0.5 * (up.mx * up.mx + up.my * up.my) / up.rho;
+    const double pe = (g - 1.0) * (up.E - kin);
+    if (!isfinite(pe) || !isfinite(p0)) ++mis_nf;
+    else mis = umax64(mis, okey(fabs(p0 - pe)));
+  }
+  ECG_RED_ADD_I(st->floor_count, floor_count);
+  ECG_RED_ADD_I(st->k_nonfinite, knf);
+  ECG_RED_MIN(st->trial_rho_min_key, rho_min);
+  ECG_RED_MAX(st->mismatch_before_key, mis);
+  ECG_RED_ADD_I(st->mismatch_before_nonfinite, mis_nf);
+}
+
+// ---- faces ------------------------------------------------------------------------
+
+// Face enthalpies h_hat (mode 0) or energy fluxes h_hat * m_hat (mode 1) of
+// every x-face (nx+1 per row) and y-face (ny+1 per column).
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_face_kernel(const EcgImexMap m, const double* __restrict__ S,
+                                                       const double* __restrict__ p, const double* __restrict__ K,
+                                                       double* __restrict__ fxv, double* __restrict__ fyv,
+                                                       unsigned char* __restrict__ fxf, unsigned char* __restrict__ fyf,
+                                                       const int mode)
+{
+  const long long nfx = static_cast<long long>(m.nx + 1) * m.ny;
+  const long long nfy = static_cast<long long>(m.nx) * (m.ny + 1);
+  for (long long f = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; f < nfx + nfy;
+       f += static_cast<long long>(gridDim.x) * NT) {
+    if (f < nfx) {
+      const int fi = static_cast<int>(f % (m.nx + 1)), j = static_cast<int>(f / (m.nx + 1));
+      const FaceOut o = face_detail(m, S, p, K, fi - 1, j, fi, j, 0);
+      fxv[f] = mode ? o.flux : o.h_hat;
+      if (fxf) fxf[f] = static_cast<unsigned char>(o.flags);
+    } else {
+      const long long g = f - nfx;
+      const int i = static_cast<int>(g % m.nx), fj = static_cast<int>(g / m.nx);
+      const FaceOut o = face_detail(m, S, p, K, i, fj - 1, i, fj, 1);
+      fyv[g] = mode ? o.flux : o.h_hat;
+      if (fyf) fyf[g] = static_cast<unsigned char>(o.flags);
+    }
+  }
+}
+
+// ---- pressure rows -------------------------------------------------------------------
+
+struct RowTerms {
+  int n;
+  int col[11];
+  double val[11];
+};
+
+// The eleven lhs terms of source_map_pressure_row_data
+// (imex_source_map_helpers.hpp:533-543) with boundary-mapped columns; terms
+// whose column is a fixed (Dirichlet) pressure are left out (they go to the
+// rhs).  Then zero terms are dropped, duplicate columns summed in insertion
+// order and the entries sorted by column, as setFromTriplets stores the row
+// (imex_source_map_step.hpp:20-36).
+__device__ __forceinline__ void row_terms(const EcgImexMap& m, const double* __restrict__ hx,
+                                          const double* __restrict__ hy, double xc, double yc, int i, int j,
+                                          RowTerms& t)
+{
+  const double he = hx[static_cast<long long>(j) * (m.nx + 1) + i + 1];
+  const double hw = hx[static_cast<long long>(j) * (m.nx + 1) + i];
+  const double hn = hy[static_cast<long long>(j + 1) * m.nx + i];
+  const double hs = hy[static_cast<long long>(j) * m.nx + i];
+  const int ci[11] = {i, i + 2, i + 1, i, i - 1, i - 2, i, i, i, i, i};
+  const int cj[11] = {j, j, j, j, j, j, j + 2, j + 1, j, j - 1, j - 2};
+  const double cv[11] = {1.0 / (m.gamma - 1.0), -xc * he, -xc * (he - hw), xc * (he + hw), xc * (he - hw),
+                         -xc * hw, -yc * hn, -yc * (hn - hs), yc * (hn + hs), yc * (hn - hs), -yc * hs};
+  t.n = 0;
+  for (int q = 0; q < 11; ++q) {
+    if (m.bubble && !m.px && ci[q] < 0) continue;
+    if (cv[q] == 0.0) continue;
+    const int c = prow(m, ci[q], cj[q]);
+    int found = -1;
+    for (int s = 0; s < t.n; ++s)
+      if (t.col[s] == c) found = s;
+    if (found >= 0) {
+      t.val[found] = t.val[found] + cv[q];
+    } else {
+      t.col[t.n] = c;
+      t.val[t.n] = cv[q];
+      ++t.n;
+    }
+  }
+  for (int a = 1; a < t.n; ++a) {  // insertion sort by column
+    const int c = t.col[a];
+    const double v = t.val[a];
+    int b = a - 1;
+    while (b >= 0 && t.col[b] > c) {
+      t.col[b + 1] = t.col[b];
+      t.val[b + 1] = t.val[b];
+      --b;
+    }
+    t.col[b + 1] = c;
+    t.val[b + 1] = v;
+  }
+}
+
+// Right-hand side of source_map_pressure_row_data
+// (imex_source_map_helpers.hpp:488-570) with its nonfinite count, plus the
+// matrix diagnostics of the Picard loop (imex_source_map_step.hpp:466-489):
+// stored entries, widest row, largest |a_ij|, max |A - A^T|.
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_rhs_kernel(const EcgImexMap m, const double* __restrict__ S,
+                                                      const double* __restrict__ K, const double* __restrict__ hx,
+                                                      const double* __restrict__ hy, const double dt, const double idx,
+                                                      const double idy, const int matrix_diag, double* __restrict__ rhs,
+                                                      EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  const double gm1 = m.gamma - 1.0;
+  const double xc = 0.25 * dt * dt * idx * idx, yc = 0.25 * dt * dt * idy * idy;
+  long long nonfinite = 0, nnz = 0;
+  unsigned long long width = 0, amax = okey(0.0), sym = okey(0.0), bmax = okey(0.0);
+  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
+       r += static_cast<long long>(gridDim.x) * NT) {
+    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+    const double he = hx[static_cast<long long>(j) * (m.nx + 1) + i + 1];
+    const double hw = hx[static_cast<long long>(j) * (m.nx + 1) + i];
+    const double hn = hy[static_cast<long long>(j + 1) * m.nx + i];
+    const double hs = hy[static_cast<long long>(j) * m.nx + i];
+    int rnf = 0;
+    double b = 0.0;
+    if (!isfinite(he) || !isfinite(hw) || !isfinite(hn) || !isfinite(hs)) ++rnf;
+    {
+      const int ci[11] = {i, i + 2, i + 1, i, i - 1, i - 2, i, i, i, i, i};
+      const double cv[11] = {1.0 / gm1, -xc * he, -xc * (he - hw), xc * (he + hw), xc * (he - hw),
+                             -xc * hw, -yc * hn, -yc * (hn - hs), yc * (hn + hs), yc * (hn - hs), -yc * hs};
+#pragma unroll
+      for (int q = 0; q < 11; ++q) {
+        if (m.bubble && !m.px && ci[q] < 0) {
+          const double c = -cv[q] * m.p_fixed;
+          b += c;
+          if (!isfinite(c)) ++rnf;
+        } else if (!isfinite(cv[q])) {
+          ++rnf;
+        }
+      }
+    }
+    const Cons s = star_at(m, S, i, j);
+    double k0, k1;
+    m_at(m, K, i, j, k0, k1);
+    const double kin = 0.5 * (k0 * k0 + k1 * k1) / s.rho;
+    double v;
+    v = s.E;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    v = -kin;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    v = -0.5 * dt * idx * he * state_b(m, S, i + 1, j).mx;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    v = -0.5 * dt * idx * (he - hw) * s.mx;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    v = 0.5 * dt * idx * hw * state_b(m, S, i - 1, j).mx;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    v = -0.5 * dt * idy * hn * state_b(m, S, i, j + 1).my;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    v = -0.5 * dt * idy * (hn - hs) * s.my;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    v = 0.5 * dt * idy * hs * state_b(m, S, i, j - 1).my;
+    if (!isfinite(v)) ++rnf;
+    b += v;
+    if (!isfinite(b)) ++rnf;
+    rhs[r] = b;
+    nonfinite += rnf;
+    if (isfinite(b)) bmax = umax64(bmax, okey(fabs(b)));
+    else bmax = okey(kInf);
+    if (matrix_diag) {
+      RowTerms t;
+      row_terms(m, hx, hy, xc, yc, i, j, t);
+      nnz += t.n;
+      width = umax64(width, static_cast<unsigned long long>(t.n));
+      for (int q = 0; q < t.n; ++q) {
+        amax = umax64(amax, okey(fabs(t.val[q])));
+        // matching entry of the transpose: row t.col[q], column r
+        const int ci2 = t.col[q] % m.nx, cj2 = t.col[q] / m.nx;
+        RowTerms u2;
+        row_terms(m, hx, hy, xc, yc, ci2, cj2, u2);
+        double tv = 0.0;
+        for (int s2 = 0; s2 < u2.n; ++s2)
+          if (u2.col[s2] == static_cast<int>(r)) tv = u2.val[s2];
+        sym = umax64(sym, okey(fabs(t.val[q] - tv)));
+      }
+    }
+  }
+  ECG_RED_ADD_I(st->row_nonfinite, nonfinite);
+  ECG_RED_ADD_I(st->nnz, nnz);
+  ECG_RED_MAX(st->max_row_width, width);
+  ECG_RED_MAX(st->abs_max_key, amax);
+  ECG_RED_MAX(st->sym_key, sym);
+  ECG_RED_MAX(st->rhs_linf_key, bmax);
+}
+
+// ---- p update and eq54 momentum -----------------------------------------------------------
+
+// p <- x with the Picard delta statistics (imex_source_map_step.hpp:536-547).
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_p_update_kernel(long long n, double* __restrict__ p,
+                                                           const double* __restrict__ x, EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  unsigned long long dl = okey(0.0), pm = okey(1.0);
+  double d2 = 0.0;
+  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
+       r += static_cast<long long>(gridDim.x) * NT) {
+    const double o = p[r], nv = x[r];
+    const double d = nv - o;
+    dl = umax64(dl, okey(fabs(d)));
+    d2 += d * d;
+    pm = umax64(pm, umax64(okey(fabs(o)), okey(fabs(nv))));
+    p[r] = nv;
+  }
+  ECG_RED_MAX(st->delta_linf_key, dl);
+  ECG_RED_ADD_D(st->delta_l2_sum, d2);
+  ECG_RED_MAX(st->pmax_key, pm);
+}
+
+// source_map_eq54_corrected_momentum_field with the physical-boundary
+// pressure (imex_source_map_helpers.hpp:249-268,334-346) and its nonfinite
+// count (:348-357).
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_momentum_kernel(const EcgImexMap m, const double* __restrict__ S,
+                                                           const double* __restrict__ p, const double dt,
+                                                           const double idx, const double idy, double* __restrict__ K,
+                                                           EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  long long nf = 0;
+  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
+       r += static_cast<long long>(gridDim.x) * NT) {
+    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+    const double gx = 0.5 * (p_b(m, p, i + 1, j) - p_b(m, p, i - 1, j)) * idx;
+    const double gy = 0.5 * (p_b(m, p, i, j + 1) - p_b(m, p, i, j - 1)) * idy;
+    const double k0 = S[r + n] - dt * gx, k1 = S[r + 2 * n] - dt * gy;
+    K[r] = k0;
+    K[r + n] = k1;
+    if (!isfinite(k0) || !isfinite(k1)) ++nf;
+  }
+  ECG_RED_ADD_I(st->k_nonfinite, nf);
+}
+
+// ---- closeout ------------------------------------------------------------------------
+
+// evaluate_source_map_final (imex_source_map_step.hpp:75-188): the
+// conservative enthalpy-flux energy closeout and its statistics.  Writes the
+// candidate state U^{n+1} = (rho*, K, E) into `out` (pitched state layout).
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_closeout_kernel(const EcgImexMap m, const EcgGrid G,
+                                                           const double* __restrict__ S, const double* __restrict__ p,
+                                                           const double* __restrict__ K, const double* __restrict__ fx,
+                                                           const double* __restrict__ fy,
+                                                           const unsigned char* __restrict__ fxf,
+                                                           const unsigned char* __restrict__ fyf, const double dt,
+                                                           double* __restrict__ out, EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  const double gm1 = m.gamma - 1.0, idx = G.inv_dx, idy = G.inv_dy;
+  long long guard = 0, hnf = 0, fnf = 0, nfc = 0, dfail = 0, pfail = 0, ifail = 0, rcount = 0;
+  unsigned long long flinf = okey(0.0);
+  unsigned long long dmin = okey(kInf), spmin = okey(kInf), spmax = okey(-kInf), epmin = okey(kInf),
+                     epmax = okey(-kInf), iemin = okey(kInf), iemax = okey(-kInf);
+  unsigned long long mcl = okey(0.0), ecl = okey(0.0), fdl = okey(0.0), rl = okey(0.0), rrel = okey(0.0),
+                     ml = okey(0.0), mrel = okey(0.0);
+  double rsum = 0.0, msum = 0.0, esum = 0.0;
+  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
+       r += static_cast<long long>(gridDim.x) * NT) {
+    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+    const long long xe = static_cast<long long>(j) * (m.nx + 1) + i + 1, xw = xe - 1;
+    const long long yn = static_cast<long long>(j + 1) * m.nx + i, ys = static_cast<long long>(j) * m.nx + i;
+    const double fe = fx[xe], fw = fx[xw], fn = fy[yn], fs = fy[ys];
+    const int fl[4] = {fxf[xe], fxf[xw], fyf[yn], fyf[ys]};
+    const double fv[4] = {fe, fw, fn, fs};
+    unsigned long long cfl = okey(0.0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      guard += fl[q] & 1;
+      hnf += (fl[q] >> 1) & 1;
+      if (fl[q] & 4) ++fnf;
+      else cfl = umax64(cfl, okey(fabs(fv[q])));
+    }
+    flinf = umax64(flinf, cfl);
+    const Cons s{S[r], S[r + n], S[r + 2 * n], S[r + 3 * n]};
+    const double m0 = K[r], m1 = K[r + n];
+    const double pr = p[r];
+    const double div = (fe - fw) * idx + (fn - fs) * idy;
+    const double en = s.E - dt * div;
+    const double kin = 0.5 * (m0 * m0 + m1 * m1) / s.rho;
+    const double ie = en - kin;
+    const double pe = gm1 * ie;
+    const double res = pr / gm1 - en + kin;
+    const double mis = pr - pe;
+    const double rs = smax(smax(smax(fabs(pr) / gm1, fabs(en)), fabs(kin)), 1.0);
+    const double ms = smax(smax(smax(fabs(pr), fabs(pe)), fabs(kin)), 1.0);
+    const long long o = static_cast<long long>(j) * G.pitch + i;
+    out[o] = s.rho;
+    out[o + G.plane] = m0;
+    out[o + 2 * G.plane] = m1;
+    out[o + 3 * G.plane] = en;
+    const bool nfb = !isfinite(s.rho) || !isfinite(m0) || !isfinite(m1) || !isfinite(en) || !isfinite(pr) ||
+                     !isfinite(kin) || !isfinite(ie) || !isfinite(pe) || !isfinite(res) || !isfinite(div);
+    if (nfb) {
+      ++nfc;
+      continue;
+    }
+    dmin = umin64(dmin, okey(s.rho));
+    spmin = umin64(spmin, okey(pr));
+    spmax = umax64(spmax, okey(pr));
+    epmin = umin64(epmin, okey(pe));
+    epmax = umax64(epmax, okey(pe));
+    iemin = umin64(iemin, okey(ie));
+    iemax = umax64(iemax, okey(ie));
+    mcl = umax64(mcl, okey(sqrt((m0 - s.mx) * (m0 - s.mx) + (m1 - s.my) * (m1 - s.my))));
+    const double ed = fabs(en - s.E);
+    ecl = umax64(ecl, okey(ed));
+    fdl = umax64(fdl, okey(fabs(div)));
+    if (s.rho <= 0.0) ++dfail;
+    if (pr <= 0.0 || pe <= 0.0) ++pfail;
+    if (ie <= 0.0) ++ifail;
+    rsum += fabs(res);
+    msum += fabs(mis);
+    esum += ed;
+    rl = umax64(rl, okey(fabs(res)));
+    rrel = umax64(rrel, okey(fabs(res) / rs));
+    ml = umax64(ml, okey(fabs(mis)));
+    mrel = umax64(mrel, okey(fabs(mis) / ms));
+    ++rcount;
+  }
+  ECG_RED_ADD_I(st->guard, guard);
+  ECG_RED_ADD_I(st->h_nonfinite, hnf);
+  ECG_RED_ADD_I(st->flux_nonfinite, fnf);
+  ECG_RED_ADD_I(st->final_nonfinite, nfc);
+  ECG_RED_ADD_I(st->density_fail, dfail);
+  ECG_RED_ADD_I(st->pressure_fail, pfail);
+  ECG_RED_ADD_I(st->ie_fail, ifail);
+  ECG_RED_ADD_I(st->residual_count, rcount);
+  ECG_RED_MAX(st->flux_linf_key, flinf);
+  ECG_RED_MIN(st->density_min_key, dmin);
+  ECG_RED_MIN(st->solved_p_min_key, spmin);
+  ECG_RED_MAX(st->solved_p_max_key, spmax);
+  ECG_RED_MIN(st->eos_p_min_key, epmin);
+  ECG_RED_MAX(st->eos_p_max_key, epmax);
+  ECG_RED_MIN(st->ie_min_key, iemin);
+  ECG_RED_MAX(st->ie_max_key, iemax);
+  ECG_RED_MAX(st->momentum_corr_key, mcl);
+  ECG_RED_MAX(st->energy_corr_key, ecl);
+  ECG_RED_MAX(st->flux_div_key, fdl);
+  ECG_RED_MAX(st->res_linf_key, rl);
+  ECG_RED_MAX(st->res_rel_key, rrel);
+  ECG_RED_MAX(st->mis_linf_key, ml);
+  ECG_RED_MAX(st->mis_rel_key, mrel);
+  ECG_RED_ADD_D(st->res_sum, rsum);
+  ECG_RED_ADD_D(st->mis_sum, msum);
+  ECG_RED_ADD_D(st->energy_sum, esum);
+}
+
+// eq 78 divergence of the final velocity (imex_source_map_step.hpp:190-224),
+// velocities looked up through the pressure index map.
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_eq78_kernel(const EcgImexMap m, const EcgGrid G,
+                                                       const double* __restrict__ S, const double* __restrict__ K,
+                                                       EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  const double idx = G.inv_dx, idy = G.inv_dy;
+  long long cnt = 0;
+  unsigned long long dl = okey(0.0), ds = okey(0.0);
+  auto vel = [&](int i, int j, int axis) {
+    const long long r = prow(m, i, j);
+    const double rho = S[r];
+    const double mm = axis == 0 ? K[r] : K[r + n];
+    if (!isfinite(rho) || rho == 0.0 || !isfinite(mm)) return __longlong_as_double(0x7ff8000000000000LL);
+    return mm / rho;
+  };
+  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
+       r += static_cast<long long>(gridDim.x) * NT) {
+    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+    const double ue = vel(i + 1, j, 0), uw = vel(i - 1, j, 0), vn = vel(i, j + 1, 1), vs = vel(i, j - 1, 1);
+    const double dv = 0.5 * (ue - uw) * idx + 0.5 * (vn - vs) * idy;
+    // std::max({...}) keeps the first of equal maxima and skips NaN only in
+    // the positions compare() allows; the values here are finite or NaN-free.
+    double sc = fabs(ue);
+    sc = (sc < fabs(uw)) ? fabs(uw) : sc;
+    sc = (sc < fabs(vn)) ? fabs(vn) : sc;
+    sc = (sc < fabs(vs)) ? fabs(vs) : sc;
+    sc = (sc < 1.0) ? 1.0 : sc;
+    const double den = sc * smax(idx, idy);
+    if (!isfinite(dv) || !isfinite(den) || den <= 0.0) continue;
+    dl = umax64(dl, okey(fabs(dv)));
+    ds = umax64(ds, okey(fabs(dv) / den));
+    ++cnt;
+  }
+  ECG_RED_ADD_I(st->eq78_count, cnt);
+  ECG_RED_MAX(st->eq78_key, dl);
+  ECG_RED_MAX(st->eq78_scaled_key, ds);
+}
+
+// Old-state loads with the IMEX step's ghost policy.
+__device__ __forceinline__ Cons old_cell(const EcgFvParams& P, const double* __restrict__ u, int i, int j)
+{
+  const int nx = P.g.nx, ny = P.g.ny;
+  if (static_cast<unsigned>(i) >= static_cast<unsigned>(nx) || static_cast<unsigned>(j) >= static_cast<unsigned>(ny)) {
+    if (i < 0) {
+      if (P.bc.x_lo == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+      i = P.bc.x_lo == BC_PERIODIC ? wrapi(i, nx) : 0;
+    } else if (i >= nx) {
+      i = P.bc.x_hi == BC_PERIODIC ? wrapi(i, nx) : nx - 1;
+    }
+    bool flip = false;
+    if (j < 0) {
+      if (P.bc.y_lo == BC_PERIODIC) {
+        j = wrapi(j, ny);
+      } else if (P.bc.y_lo == BC_REFLECT) {
+        j = -j - 1;
+        j = j > ny - 1 ? ny - 1 : j;
+        flip = true;
+      } else {
+        j = 0;
+      }
+    } else if (j >= ny) {
+      j = P.bc.y_hi == BC_PERIODIC ? wrapi(j, ny) : ny - 1;
+    }
+    const long long o = static_cast<long long>(j) * P.g.pitch + i;
+    Cons c{u[o], u[o + P.g.plane], u[o + 2 * P.g.plane], u[o + 3 * P.g.plane]};
+    if (flip) c.my = -c.my;
+    return c;
+  }
+  const long long o = static_cast<long long>(j) * P.g.pitch + i;
+  return Cons{u[o], u[o + P.g.plane], u[o + 2 * P.g.plane], u[o + 3 * P.g.plane]};
+}
+
+#undef ECG_RED_MAX
+#undef ECG_RED_MIN
+#undef ECG_RED_ADD_I
+#undef ECG_RED_ADD_D
+
+inline int blocks_for(long long n, int nt)
+{
+  long long b = (n + nt - 1) / nt;
+  if (b > 148 * 8) b = 148 * 8;
+  return static_cast<int>(b < 1 ? 1 : b);
+}
+
+}  // namespace imexk
+
+// ---- launchers ---------------------------------------------------------------------------
+
+inline cudaError_t imex_star(const EcgFvParams& P, const double* u, double dt, double* S, double* p, double* K,
+                             EcgImexStats* st, cudaStream_t s)
+{
+  const long long n = static_cast<long long>(P.g.nx) * P.g.ny;
+  imexk::imex_star_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(P, u, dt, S, p, K, st);
+  return cudaGetLastError();
+}
+
+inline cudaError_t imex_faces(const EcgImexMap& m, const double* S, const double* p, const double* K, double* fx,
+                              double* fy, unsigned char* fxf, unsigned char* fyf, int mode, cudaStream_t s)
+{
+  const long long n = static_cast<long long>(m.nx + 1) * m.ny + static_cast<long long>(m.nx) * (m.ny + 1);
+  imexk::imex_face_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, p, K, fx, fy, fxf, fyf, mode);
+  return cudaGetLastError();
+}
+
+inline cudaError_t imex_rhs(const EcgImexMap& m, const double* S, const double* K, const double* hx, const double* hy,
+                            double dt, double idx, double idy, int matrix_diag, double* rhs, EcgImexStats* st,
+                            cudaStream_t s)
+{
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  imexk::imex_rhs_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, K, hx, hy, dt, idx, idy, matrix_diag,
+                                                                         rhs, st);
+  return cudaGetLastError();
+}
+
+inline cudaError_t imex_p_update(long long n, double* p, const double* x, EcgImexStats* st, cudaStream_t s)
+{
+  imexk::imex_p_update_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(n, p, x, st);
+  return cudaGetLastError();
+}
+
+inline cudaError_t imex_momentum(const EcgImexMap& m, const double* S, const double* p, double dt, double idx,
+                                 double idy, double* K, EcgImexStats* st, cudaStream_t s)
+{
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  imexk::imex_momentum_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, p, dt, idx, idy, K, st);
+  return cudaGetLastError();
+}
+
+inline cudaError_t imex_closeout(const EcgImexMap& m, const EcgGrid& G, const double* S, const double* p,
+                                 const double* K, const double* fx, const double* fy, const unsigned char* fxf,
+                                 const unsigned char* fyf, double dt, double* out, EcgImexStats* st, cudaStream_t s)
+{
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  imexk::imex_closeout_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, G, S, p, K, fx, fy, fxf, fyf, dt, out,
+                                                                              st);
+  return cudaGetLastError();
+}
+
+inline cudaError_t imex_eq78(const EcgImexMap& m, const EcgGrid& G, const double* S, const double* K, EcgImexStats* st,
+                             cudaStream_t s)
+{
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  imexk::imex_eq78_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, G, S, K, st);
+  return cudaGetLastError();
+}
+
+}  // namespace ECG_NS
