@@ -179,11 +179,12 @@ bool reduce_state(ecg_ctx* c)
 bool fetch_fused(ecg_ctx* c)
 {
   if (!c->fused_pending) return true;
-  if (!cuda_ok(c, cudaMemcpyAsync(c->h_stats, c->d_stats, 2 * sizeof(EcgStepStats), cudaMemcpyDeviceToHost, c->stream),
+  if (!cuda_ok(c, cudaMemcpyAsync(c->h_stats, c->d_stats + c->fused_slot, sizeof(EcgStepStats),
+                                  cudaMemcpyDeviceToHost, c->stream),
                "copy stats"))
     return false;
   if (!cuda_ok(c, cudaStreamSynchronize(c->stream), "sync")) return false;
-  const EcgStepStats& s = c->h_stats[1];
+  const EcgStepStats& s = c->h_stats[0];
   c->fused_max_rate = okey_to_double(s.max_rate_key);
   c->fused_rho_min = okey_to_double(s.rho_min_key);
   c->fused_p_min = okey_to_double(s.p_min_key);
@@ -359,7 +360,9 @@ ecg_status ecg_create(ecg_ctx** out, const ecg_run_config* cfg, const ecg_gpu_op
   c->grid.inv_dy = 1.0 / c->grid.dy;
   c->grid.plo_x = cfg->prob_lo[0];
   c->grid.plo_y = cfg->prob_lo[1];
-  c->tile_y = (o.tile_y == 8) ? 8 : 16;
+  // kernel choice: 0 default (fast build: column-strip marching kernel; exact
+  // build: 32x16 tile), 1 square 16x16 tile (fast build), 8 or 16: 32xTY tile
+  c->tile_y = (o.tile_y == 1 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
   const size_t sbytes = sizeof(double) * 4 * c->grid.plane;
   bool ok = true;
   if (o.stream) {
@@ -376,7 +379,7 @@ ecg_status ecg_create(ecg_ctx** out, const ecg_run_config* cfg, const ecg_gpu_op
   const size_t rbytes = sizeof(double) * 4 * static_cast<size_t>(nx + 4) * (ny + 4);
   ok = ok && cuda_ok(c, cudaMalloc(&c->d_ring, rbytes), "alloc ring");
   ok = ok && cuda_ok(c, cudaMemsetAsync(c->d_ring, 0, rbytes, c->stream), "memset");
-  c->stats_cap = ecg_ctx::kChunk + 1;
+  c->stats_cap = ecg_ctx::kChunk + 1;  // >= 3 host-mode slots
   ok = ok && cuda_ok(c, cudaMalloc(&c->d_stats, sizeof(EcgStepStats) * c->stats_cap), "alloc stats");
   ok = ok && cuda_ok(c, cudaMallocHost(&c->h_stats, sizeof(EcgStepStats) * c->stats_cap), "alloc host stats");
   ok = ok && cuda_ok(c, cudaMalloc(&c->d_state_stats, sizeof(EcgStateStats)), "alloc state stats");
@@ -482,23 +485,35 @@ ecg_status ecg_euler_fv_one_step(ecg_ctx* c, double dt, double time, int32_t* de
   if (!c) return ECG_ERR_BAD_ARG;
   if (!c->uploaded) return ECG_ERR_NOT_READY;
   const EcgFvParams p = fv_params(c, false);
+  // Host-dt launches rotate over three stats records: launch n accumulates
+  // into (n+1)%3 and re-initialises (n+2)%3 for launch n+1, so one launch is
+  // the whole step.
+  if (!c->host_slots_ready) {
+    if (!cuda_ok(c, c->ops->init_stats(c->d_stats, 3, time, c->stream), "init stats")) return ECG_ERR_CUDA;
+    c->host_slots_ready = true;
+    c->host_step = 0;
+  }
   EcgDtCtl ctl;
   std::memset(&ctl, 0, sizeof(ctl));
   ctl.device_dt = 0;
   ctl.dt = dt;
   ctl.time = time;
   ctl.count_degenerate = c->cfg.riemann != ECG_RIEMANN_RUSANOV;
-  if (!cuda_ok(c, c->ops->init_stats(c->d_stats, 2, time, c->stream), "init stats")) return ECG_ERR_CUDA;
+  ctl.read_slot = static_cast<int>(c->host_step % 3);
+  ctl.acc_slot = static_cast<int>((c->host_step + 1) % 3);
+  ctl.reset_slot = static_cast<int>((c->host_step + 2) % 3);
   if (!fill_ring(c, c->cur_state(), time, nullptr, 0)) return ECG_ERR_CUDA;
-  if (!cuda_ok(c, c->ops->fv_step(p, c->cur_state(), c->next_state(), c->d_stats, 0, ctl, c->tile_y, c->stream),
+  if (!cuda_ok(c, c->ops->fv_step(p, c->cur_state(), c->next_state(), c->d_stats, ctl, c->tile_y, c->stream),
                "fv_step"))
     return ECG_ERR_CUDA;
   c->cur ^= 1;
+  ++c->host_step;
   // The fused epilogue reduced compute_euler_dt / compute_diagnostics over the
-  // new state into d_stats[1]: those calls read it instead of a second pass.
+  // new state into d_stats[acc_slot]: those calls read it instead of a second pass.
   c->state_stats_valid = false;
   c->fused_valid = false;
   c->fused_pending = true;
+  c->fused_slot = ctl.acc_slot;
   if (degenerate) {
     if (!fetch_fused(c)) return ECG_ERR_CUDA;
     *degenerate = c->fused_degenerate;
@@ -601,6 +616,7 @@ static ecg_status run_explicit(ecg_ctx* c, int32_t max_step, double stop_time, e
   out->dt_min = std::numeric_limits<double>::infinity();
   const EcgFvParams p = fv_params(c, false);
   const int K = ecg_ctx::kChunk;
+  c->host_slots_ready = false;
   double t = 0.0;
   int steps = 0;
   // stats[0] <- reductions of the initial state (compute_diagnostics before
@@ -618,6 +634,7 @@ static ecg_status run_explicit(ecg_ctx* c, int32_t max_step, double stop_time, e
     ctl.device_dt = 1;
     ctl.max_step = max_step;
     ctl.count_degenerate = c->cfg.riemann != ECG_RIEMANN_RUSANOV;
+    ctl.reset_slot = -1;
     ctl.cfl = c->cfg.cfl;
     ctl.stop_time = stop_time;
     // capture (or reuse) the chunk graph for this buffer parity and step base
@@ -637,7 +654,10 @@ static ecg_status run_explicit(ecg_ctx* c, int32_t max_step, double stop_time, e
         const double* in = c->d_state[(c->cur + k) & 1];
         double* o = c->d_state[(c->cur + k + 1) & 1];
         fill_ring(c, in, 0.0, c->d_stats, k);
-        c->ops->fv_step(p, in, o, c->d_stats, k, ctl, c->tile_y, c->stream);
+        EcgDtCtl kc = ctl;
+        kc.read_slot = k;
+        kc.acc_slot = k + 1;
+        c->ops->fv_step(p, in, o, c->d_stats, kc, c->tile_y, c->stream);
       }
       const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
       if (!cuda_ok(c, ce, "end capture")) return ECG_ERR_CUDA;

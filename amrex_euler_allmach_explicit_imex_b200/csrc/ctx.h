@@ -42,6 +42,10 @@ struct ecg_ctx {
   bool fused_pending = false;  // they are still in d_stats[1] on the device
   double fused_max_rate = 0.0, fused_rho_min = 0.0, fused_p_min = 0.0;
   int fused_nonfinite = 0, fused_degenerate = 0;
+  int fused_slot = 1;
+  // host-dt launches: rotating stats records (see ecg_euler_fv_one_step)
+  bool host_slots_ready = false;
+  long long host_step = 0;
 
   struct Graph {
     int cur = 0;
@@ -57,7 +61,12 @@ struct ecg_ctx {
   const double* cur_state() const { return d_state[cur]; }
   double* cur_state_mut() { return d_state[cur]; }
   double* next_state() { return d_state[cur ^ 1]; }
-  void invalidate() { fused_valid = false; fused_pending = false; state_stats_valid = false; }
+  void invalidate()
+  {
+    fused_valid = false;
+    fused_pending = false;
+    state_stats_valid = false;
+  }
   ~ecg_ctx();
 };
 

@@ -76,7 +76,7 @@ __device__ __forceinline__ Cons pflux(const Prim& q, const Cons& u, int axis)
 }
 
 // rusanov_flux, reconstruction_fluxes.hpp:82-92
-__device__ __noinline__ Cons rusanov_flux(const Prim& l, const Prim& r, int axis, double g)
+static __device__ __noinline__ Cons rusanov_flux(const Prim& l, const Prim& r, int axis, double g)
 {
   const Cons ul = to_cons(l, g), ur = to_cons(r, g);
   const Cons fl = pflux(l, ul, axis), fr = pflux(r, ur, axis);
@@ -155,7 +155,7 @@ __device__ __forceinline__ double clamp01(double v) { return smin(smax(v, 0.0), 
 // xie_am_hllc_p_flux, reconstruction_fluxes.hpp:254-371.  `degenerate` is the
 // HLLC degeneracy of the same (uncorrected) states, as
 // count_hllc_degenerate_star_states evaluates it (explicit_update.hpp:17-50).
-__device__ __noinline__ Cons xie_flux(const Prim& l, const Prim& r, int axis, double g, double sensor, bool& degenerate)
+static __device__ __noinline__ Cons xie_flux(const Prim& l, const Prim& r, int axis, double g, double sensor, bool& degenerate)
 {
   const double ql = normal_vel(l, axis), qr = normal_vel(r, axis);
   const double pl = l.p, pr = r.p;

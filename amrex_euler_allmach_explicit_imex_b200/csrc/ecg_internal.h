@@ -74,9 +74,12 @@ struct EcgStepStats {
 
 // dt control of one explicit launch.
 struct EcgDtCtl {
-  int device_dt;      // 0: use dt/time below; 1: compute dt from stats[k] like compute_euler_dt
+  int device_dt;      // 0: use dt/time below; 1: compute dt from stats[read_slot] like compute_euler_dt
   int max_step;       // device mode: loop step limit
   int count_degenerate;
+  int read_slot;      // device mode: record of the state this launch advances
+  int acc_slot;       // record receiving the reductions of the new state
+  int reset_slot;     // record this launch re-initialises for the next one (-1: none)
   double dt, time;    // host mode
   double cfl, stop_time;
 };
@@ -98,7 +101,7 @@ struct EcgStateStats {
 
 // Function table of one arithmetic build of the stencil kernels.
 struct EcgStencilOps {
-  cudaError_t (*fv_step)(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, int k,
+  cudaError_t (*fv_step)(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
                          const EcgDtCtl& ctl, int tile_y, cudaStream_t s);
   cudaError_t (*state_reduce)(const EcgFvParams& p, const double* u, int eq79, EcgStateStats* out, cudaStream_t s);
   cudaError_t (*ghost_box)(const EcgFvParams& p, const EcgProblem& pr, const double* u, double time,

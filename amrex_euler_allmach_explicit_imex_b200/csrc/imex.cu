@@ -1,18 +1,429 @@
-// IMEX T1/S2 BDLTV20 source-map step (placeholder until the IMEX kernels land).
-#include "ctx.h"
+// euler_imex_bdltv20_o1_source_map_picard_one_step on the device
+// (imex/imex_source_map_step.hpp:300-616): star update -> Picard iterations
+// {face enthalpies, pressure-row rhs, GMRES, gate, p <- x, eq54 momentum} ->
+// conservative closeout.  The state stays on the device; the host reads the
+// per-phase reductions (a few hundred bytes) to take the reference's
+// early-return decisions.
+#include <cuda_runtime.h>
 
-struct EcgImexState {};
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "ctx.h"
+#include "imex_internal.h"
+
+struct EcgImexState {
+  long long n = 0;
+  int max_iter = 0;
+  bool mixed = false;
+  double* S = nullptr;   // star state, 4 compact planes
+  double* p = nullptr;   // Picard pressure
+  double* K = nullptr;   // lagged momentum, 2 planes
+  double* hx = nullptr;  // x-face enthalpy / energy flux, (nx+1) x ny
+  double* hy = nullptr;  // y-face, nx x (ny+1)
+  double* fx = nullptr;
+  double* fy = nullptr;
+  unsigned char* fxf = nullptr;
+  unsigned char* fyf = nullptr;
+  double* rhs = nullptr;
+  double* x = nullptr;
+  EcgImexStats* d_st = nullptr;
+  EcgImexStats* h_st = nullptr;  // pinned
+  EcgImexStats init{};           // reset template
+  EcgGmresWork* gw = nullptr;
+};
+
+namespace {
+
+unsigned long long key_of(double x)
+{
+  unsigned long long b;
+  std::memcpy(&b, &x, sizeof(b));
+  return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
+}
+
+EcgImexStats stats_template()
+{
+  const double inf = std::numeric_limits<double>::infinity();
+  EcgImexStats s;
+  std::memset(&s, 0, sizeof(s));
+  s.trial_rho_min_key = key_of(inf);
+  s.mismatch_before_key = key_of(0.0);
+  s.abs_max_key = key_of(0.0);
+  s.sym_key = key_of(0.0);
+  s.rhs_linf_key = key_of(0.0);
+  s.delta_linf_key = key_of(0.0);
+  s.pmax_key = key_of(1.0);
+  s.flux_linf_key = key_of(0.0);
+  s.density_min_key = key_of(inf);
+  s.solved_p_min_key = key_of(inf);
+  s.solved_p_max_key = key_of(-inf);
+  s.eos_p_min_key = key_of(inf);
+  s.eos_p_max_key = key_of(-inf);
+  s.ie_min_key = key_of(inf);
+  s.ie_max_key = key_of(-inf);
+  s.momentum_corr_key = key_of(0.0);
+  s.energy_corr_key = key_of(0.0);
+  s.flux_div_key = key_of(0.0);
+  s.res_linf_key = key_of(0.0);
+  s.res_rel_key = key_of(0.0);
+  s.mis_linf_key = key_of(0.0);
+  s.mis_rel_key = key_of(0.0);
+  s.eq78_key = key_of(0.0);
+  s.eq78_scaled_key = key_of(0.0);
+  return s;
+}
+
+bool ensure_state(ecg_ctx* c)
+{
+  const bool mixed = c->opt.imex_precision == ECG_IMEX_MIXED;
+  const int max_iter = c->cfg.imex_solver_max_iter;
+  EcgImexState* im = c->imex;
+  if (im && im->max_iter >= max_iter && (!mixed || im->mixed)) return true;
+  imex_free(c);
+  im = new EcgImexState();
+  c->imex = im;
+  const int nx = c->grid.nx, ny = c->grid.ny;
+  const long long n = static_cast<long long>(nx) * ny;
+  im->n = n;
+  im->max_iter = max_iter;
+  im->mixed = mixed;
+  const long long nfx = static_cast<long long>(nx + 1) * ny, nfy = static_cast<long long>(nx) * (ny + 1);
+  bool ok = true;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (ok) ok = ecgi::cuda_ok(c, cudaMalloc(p, bytes), "imex alloc");
+  };
+  alloc(reinterpret_cast<void**>(&im->S), sizeof(double) * 4 * n);
+  alloc(reinterpret_cast<void**>(&im->p), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&im->K), sizeof(double) * 2 * n);
+  alloc(reinterpret_cast<void**>(&im->hx), sizeof(double) * nfx);
+  alloc(reinterpret_cast<void**>(&im->hy), sizeof(double) * nfy);
+  alloc(reinterpret_cast<void**>(&im->fx), sizeof(double) * nfx);
+  alloc(reinterpret_cast<void**>(&im->fy), sizeof(double) * nfy);
+  alloc(reinterpret_cast<void**>(&im->fxf), nfx);
+  alloc(reinterpret_cast<void**>(&im->fyf), nfy);
+  alloc(reinterpret_cast<void**>(&im->rhs), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&im->x), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&im->d_st), sizeof(EcgImexStats));
+  if (ok) ok = ecgi::cuda_ok(c, cudaMallocHost(&im->h_st, sizeof(EcgImexStats)), "imex host alloc");
+  im->init = stats_template();
+  if (ok) {
+    std::string err;
+    im->gw = gmres_work_create(n, max_iter < 1 ? 1 : max_iter, c->num_sms, c->device, mixed, &err);
+    if (!im->gw) {
+      c->err = err;
+      ok = false;
+    }
+  }
+  return ok;
+}
+
+bool reset_stats(ecg_ctx* c)
+{
+  return ecgi::cuda_ok(c, cudaMemcpyAsync(c->imex->d_st, &c->imex->init, sizeof(EcgImexStats), cudaMemcpyHostToDevice,
+                                          c->stream), "reset stats");
+}
+
+bool fetch_stats(ecg_ctx* c)
+{
+  if (!ecgi::cuda_ok(c, cudaMemcpyAsync(c->imex->h_st, c->imex->d_st, sizeof(EcgImexStats), cudaMemcpyDeviceToHost,
+                                        c->stream), "fetch stats"))
+    return false;
+  return ecgi::cuda_ok(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+double kd(unsigned long long k) { return ecgi::okey_to_double(k); }
+double finite_or_nan(double v) { return std::isfinite(v) ? v : std::numeric_limits<double>::quiet_NaN(); }
+
+EcgImexMap imex_map(ecg_ctx* c)
+{
+  EcgImexMap m;
+  std::memset(&m, 0, sizeof(m));
+  m.nx = c->grid.nx;
+  m.ny = c->grid.ny;
+  m.px = c->cfg.is_periodic[0] != 0;
+  m.py = c->cfg.is_periodic[1] != 0;
+  m.bubble = c->cfg.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D;
+  m.gamma = c->cfg.gamma;
+  // shock_density_bubble_post_shock_state, problem_initialization.hpp:51-58
+  const double q[4] = {2.8181818181818183, 1.6064386578049976, 0.0, 5.0};
+  const double kin = 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2]);
+  m.cst[0] = q[0];
+  m.cst[1] = q[0] * q[1];
+  m.cst[2] = q[0] * q[2];
+  m.cst[3] = q[3] / (c->cfg.gamma - 1.0) + kin;
+  m.p_fixed = q[3];
+  return m;
+}
+
+}  // namespace
 
 void imex_free(ecg_ctx* c)
 {
-  delete c->imex;
+  EcgImexState* im = c->imex;
+  if (!im) return;
+  cudaFree(im->S);
+  cudaFree(im->p);
+  cudaFree(im->K);
+  cudaFree(im->hx);
+  cudaFree(im->hy);
+  cudaFree(im->fx);
+  cudaFree(im->fy);
+  cudaFree(im->fxf);
+  cudaFree(im->fyf);
+  cudaFree(im->rhs);
+  cudaFree(im->x);
+  cudaFree(im->d_st);
+  cudaFreeHost(im->h_st);
+  gmres_work_destroy(im->gw);
+  delete im;
   c->imex = nullptr;
 }
 
-ecg_status imex_run(ecg_ctx*, int32_t, double, ecg_run_result*) { return ECG_ERR_UNSUPPORTED; }
-
-extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double, ecg_imex_diag*)
+extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
 {
-  if (!c) return ECG_ERR_BAD_ARG;
-  return ECG_ERR_UNSUPPORTED;
+  if (!c || !out) return ECG_ERR_BAD_ARG;
+  if (!c->uploaded) return ECG_ERR_NOT_READY;
+  if (c->cfg.spatial_order != 2) return ECG_ERR_UNSUPPORTED;
+  if (!ensure_state(c)) return ECG_ERR_CUDA;
+  EcgImexState* im = c->imex;
+  const EcgImexOps* ops = c->opt.arith == ECG_ARITH_EXACT ? &ecg_imex_exact_ops : &ecg_imex_fast_ops;
+  const bool mixed = c->opt.imex_precision == ECG_IMEX_MIXED;
+  ecg_imex_diag& d = *out;
+  std::memset(&d, 0, sizeof(d));
+  d.solver_status = ECG_SOLVER_NOT_RUN;
+  d.linear_solver_status_last = -1;
+  const double inf = std::numeric_limits<double>::infinity();
+  const EcgFvParams P = ecgi::fv_params(c, true);
+  const EcgImexMap m = imex_map(c);
+  const long long n = im->n;
+  const double idx = c->grid.inv_dx, idy = c->grid.inv_dy;
+  cudaStream_t s = c->stream;
+
+  // star update and step initialisation (imex_source_map_step.hpp:405-454)
+  if (!reset_stats(c)) return ECG_ERR_CUDA;
+  if (!ecgi::cuda_ok(c, ops->star(P, c->cur_state(), dt, im->S, im->p, im->K, im->d_st, s), "star")) return ECG_ERR_CUDA;
+  if (!fetch_stats(c)) return ECG_ERR_CUDA;
+  EcgImexStats& st = *im->h_st;
+  d.kinetic_lag_nonfinite_count = static_cast<int>(st.k_nonfinite);
+  d.trial_density_min = kd(st.trial_rho_min_key);
+  d.density_denominator_floor_count = static_cast<int>(st.floor_count);
+  if (st.floor_count > 0) {
+    d.solver_status = ECG_SOLVER_DENSITY_DENOMINATOR_FLOOR_USED;
+    d.positivity_failure_count = static_cast<int>(st.floor_count);
+    return ECG_OK;
+  }
+  d.pressure_energy_residual_before_linf = st.mismatch_before_nonfinite ? inf : kd(st.mismatch_before_key);
+
+  EcgPressureOp op;
+  std::memset(&op, 0, sizeof(op));
+  op.nx = m.nx;
+  op.ny = m.ny;
+  op.px = m.px;
+  op.py = m.py;
+  op.bubble = m.bubble;
+  op.diag0 = 1.0 / (c->cfg.gamma - 1.0);
+  op.xc = 0.25 * dt * dt * idx * idx;
+  op.yc = 0.25 * dt * dt * idy * idy;
+  op.hx = im->hx;
+  op.hy = im->hy;
+  const double tol = c->cfg.imex_solver_tol;
+
+  for (int pic = 0; pic < c->cfg.imex_picard_iterations; ++pic) {
+    // pressure system (source_map_build_pressure_system, imex_source_map_step.hpp:8-38,464-497)
+    if (!reset_stats(c)) return ECG_ERR_CUDA;
+    if (!ecgi::cuda_ok(c, ops->faces(m, im->S, im->p, im->K, im->hx, im->hy, nullptr, nullptr, 0, s), "faces"))
+      return ECG_ERR_CUDA;
+    if (!ecgi::cuda_ok(c, ops->rhs(m, im->S, im->K, im->hx, im->hy, dt, idx, idy, 1, im->rhs, im->d_st, s), "rhs"))
+      return ECG_ERR_CUDA;
+    if (!fetch_stats(c)) return ECG_ERR_CUDA;
+    d.pressure_matrix_rows = static_cast<int>(n);
+    d.pressure_matrix_nonzeros = static_cast<int>(st.nnz);
+    d.pressure_matrix_max_row_width = static_cast<int>(st.max_row_width);
+    d.kinetic_jacobian_abs_max = kd(st.abs_max_key);
+    d.pressure_matrix_symmetry_linf = kd(st.sym_key);
+    if (st.row_nonfinite > 0 || !std::isfinite(kd(st.rhs_linf_key))) {
+      d.solver_status = ECG_SOLVER_SOURCE_MAP_PRESSURE_ROW_NONFINITE;
+      d.kinetic_lag_nonfinite_count = static_cast<int>(st.row_nonfinite);
+      d.nonfinite_count = static_cast<int>(st.row_nonfinite);
+      return ECG_OK;
+    }
+    double r0 = 0.0, bn = 1.0;
+    int nf = 0;
+    if (!ecgi::cuda_ok(c, pressure_residual(im->gw, op, im->rhs, im->p, &r0, &bn, &nf, s), "initial residual"))
+      return ECG_ERR_CUDA;
+    d.solver_initial_residual = r0;
+    d.solver_initial_rhs_norm = bn;
+    EcgGmresResult g;
+    if (!ecgi::cuda_ok(c, gmres_solve(im->gw, op, im->rhs, im->p, im->x, c->cfg.imex_solver_max_iter, tol, mixed,
+                                      c->opt.mixed_inner_max_iter, c->opt.mixed_inner_rtol,
+                                      c->opt.mixed_max_refinements, &g, s),
+                       "gmres"))
+      return ECG_ERR_CUDA;
+    if (g.timeout) {
+      c->err = "gmres grid barrier timed out";
+      return ECG_ERR_TIMEOUT;
+    }
+    d.solver_iterations += g.iterations;
+    d.gmres_inner_iterations += g.inner_iterations;
+    d.gmres_refinements += g.refinements;
+    double lr = 0.0, bn2 = 1.0;
+    if (!ecgi::cuda_ok(c, pressure_residual(im->gw, op, im->rhs, im->x, &lr, &bn2, &nf, s), "linear residual"))
+      return ECG_ERR_CUDA;
+    d.pressure_linear_residual_linf = lr;
+    d.pressure_linear_residual_relative_linf = lr / d.solver_initial_rhs_norm;
+    d.solver_residual = d.pressure_linear_residual_linf;
+    d.solver_relative_residual = d.pressure_linear_residual_relative_linf;
+    const bool abs_ok = lr <= tol;
+    const bool rel_ok = d.pressure_linear_residual_relative_linf <= tol;
+    d.linear_solver_status_last = abs_ok ? ECG_SOLVER_CONVERGED_ABSOLUTE
+                                         : (rel_ok ? ECG_SOLVER_CONVERGED_RELATIVE : ECG_SOLVER_LINEAR_SOLVE_NOT_CONVERGED);
+    if (!std::isfinite(lr) || nf || g.nonfinite) {
+      if (!std::isfinite(lr) || nf) {
+        d.solver_status = ECG_SOLVER_LINEAR_RESIDUAL_NONFINITE;
+        d.nonfinite_count = 1;
+        return ECG_OK;
+      }
+    }
+    if (!abs_ok && !rel_ok) {
+      d.solver_status = g.breakdown ? ECG_SOLVER_GMRES_BREAKDOWN_NOT_CONVERGED : ECG_SOLVER_LINEAR_SOLVE_NOT_CONVERGED;
+      return ECG_OK;
+    }
+    // p <- x, eq54 momentum refresh (imex_source_map_step.hpp:536-564)
+    if (!reset_stats(c)) return ECG_ERR_CUDA;
+    if (!ecgi::cuda_ok(c, ops->p_update(n, im->p, im->x, im->d_st, s), "p update")) return ECG_ERR_CUDA;
+    if (!ecgi::cuda_ok(c, ops->momentum(m, im->S, im->p, dt, idx, idy, im->K, im->d_st, s), "momentum"))
+      return ECG_ERR_CUDA;
+    if (!fetch_stats(c)) return ECG_ERR_CUDA;
+    d.kinetic_lag_nonfinite_count = static_cast<int>(st.k_nonfinite);
+    if (st.k_nonfinite > 0) {
+      d.solver_status = ECG_SOLVER_SOURCE_MAP_LAGGED_MOMENTUM_NONFINITE;
+      d.nonfinite_count = d.kinetic_lag_nonfinite_count;
+      return ECG_OK;
+    }
+    ++d.kinetic_lag_update_count;
+    d.pressure_picard_delta_linf = kd(st.delta_linf_key);
+    d.source_picard_delta_l2_relative_to_pmax = std::sqrt(st.delta_l2_sum / static_cast<double>(n)) / kd(st.pmax_key);
+    ++d.source_picard_iterations_used;
+    ++d.picard_pressure_solves_used;
+  }
+  d.solver_status = d.linear_solver_status_last;
+
+  // conservative closeout (evaluate_source_map_final, imex_source_map_step.hpp:75-258)
+  if (!reset_stats(c)) return ECG_ERR_CUDA;
+  if (!ecgi::cuda_ok(c, ops->faces(m, im->S, im->p, im->K, im->fx, im->fy, im->fxf, im->fyf, 1, s), "faces"))
+    return ECG_ERR_CUDA;
+  double* out_state = c->next_state();
+  if (!ecgi::cuda_ok(c, ops->closeout(m, c->grid, im->S, im->p, im->K, im->fx, im->fy, im->fxf, im->fyf, dt, out_state,
+                                      im->d_st, s),
+                     "closeout"))
+    return ECG_ERR_CUDA;
+  if (!ecgi::cuda_ok(c, ops->eq78(m, c->grid, im->S, im->K, im->d_st, s), "eq78")) return ECG_ERR_CUDA;
+  if (!fetch_stats(c)) return ECG_ERR_CUDA;
+  const int rcount = static_cast<int>(st.residual_count);
+  const int nfc = static_cast<int>(st.final_nonfinite);
+  double rl1 = 0.0, ml1 = 0.0, el1 = 0.0;
+  double rlinf = kd(st.res_linf_key), rrel = kd(st.res_rel_key), mlinf = kd(st.mis_linf_key), mrel = kd(st.mis_rel_key);
+  double e78 = kd(st.eq78_key), e78s = kd(st.eq78_scaled_key);
+  if (nfc > 0 || rcount == 0) {
+    rl1 = rlinf = rrel = ml1 = mlinf = mrel = el1 = e78 = e78s = inf;
+  } else if (st.eq78_count == 0) {
+    e78 = e78s = inf;
+  } else {
+    const double ic = 1.0 / static_cast<double>(rcount);
+    rl1 = st.res_sum * ic;
+    ml1 = st.mis_sum * ic;
+    el1 = st.energy_sum * ic;
+  }
+  d.coupled_residual_l1_final = rl1;
+  d.coupled_residual_linf_final = rlinf;
+  d.coupled_residual_relative_linf_final = rrel;
+  d.pressure_energy_residual_l1 = ml1;
+  d.pressure_energy_residual_linf = mlinf;
+  d.pressure_energy_residual_relative_linf = mrel;
+  d.rho_min = finite_or_nan(kd(st.density_min_key));
+  d.pressure_min = finite_or_nan(kd(st.eos_p_min_key));
+  d.internal_energy_min = finite_or_nan(kd(st.ie_min_key));
+  d.trial_density_min = d.rho_min;
+  d.solved_pressure_min = finite_or_nan(kd(st.solved_p_min_key));
+  d.solved_pressure_max = finite_or_nan(kd(st.solved_p_max_key));
+  d.eos_pressure_min = finite_or_nan(kd(st.eos_p_min_key));
+  d.eos_pressure_max = finite_or_nan(kd(st.eos_p_max_key));
+  d.internal_energy_max = finite_or_nan(kd(st.ie_max_key));
+  d.nonfinite_count = nfc;
+  d.positivity_failure_count = static_cast<int>(st.density_fail + st.pressure_fail + st.ie_fail);
+  d.momentum_correction_linf = kd(st.momentum_corr_key);
+  d.energy_correction_linf = kd(st.energy_corr_key);
+  d.energy_closeout_delta_linf = kd(st.energy_corr_key);
+  d.energy_flux_linf = kd(st.flux_linf_key);
+  d.energy_flux_divergence_linf = kd(st.flux_div_key);
+  d.eq78_divergence_linf = e78;
+  d.eq78_divergence_scaled_linf = e78s;
+  d.energy_closeout_delta_l1 = el1;
+  d.face_enthalpy_denominator_guard_count = static_cast<int>(st.guard);
+  d.face_enthalpy_nonfinite_count = static_cast<int>(st.h_nonfinite);
+  d.energy_flux_nonfinite_count = static_cast<int>(st.flux_nonfinite);
+  // copy_source_map_eval_to_state: the step reached its end, commit U^{n+1}
+  c->cur ^= 1;
+  c->invalidate();
+  return ECG_OK;
+}
+
+// The driver loop for the IMEX method (app/driver_main.hpp:224-310).
+ecg_status imex_run(ecg_ctx* c, int32_t max_step, double stop_time, ecg_run_result* out)
+{
+  std::memset(out, 0, sizeof(*out));
+  out->dt_min = std::numeric_limits<double>::infinity();
+  const double saved_stop = c->cfg.stop_time;
+  c->cfg.stop_time = stop_time;
+  double t = 0.0;
+  int steps = 0;
+  ecg_diagnostics dg;
+  ecg_status e = ecg_compute_diagnostics(c, &dg);
+  if (e != ECG_OK) {
+    c->cfg.stop_time = saved_stop;
+    return e;
+  }
+  if (dg.nonfinite_count > 0 || dg.rho_min <= 0.0 || dg.pressure_min <= 0.0) {
+    out->failed = 1;
+    out->failure_code = ECG_FAILURE_NONFINITE_STATE;
+  }
+  while (!out->failed && steps < max_step && t < stop_time - 1.0e-14) {
+    double dt = 0.0;
+    e = ecg_compute_imex_dt(c, t, &dt, nullptr);
+    if (e != ECG_OK) break;
+    if (!std::isfinite(dt) || dt <= 0.0) {
+      out->failed = 1;
+      out->failure_code = ECG_FAILURE_INVALID_TIME_STEP;
+      break;
+    }
+    ecg_imex_diag d;
+    e = ecg_imex_step(c, dt, &d);
+    if (e != ECG_OK) break;
+    out->imex_solver_iterations_max = std::max(out->imex_solver_iterations_max, d.solver_iterations);
+    if (d.solver_status != ECG_SOLVER_CONVERGED_ABSOLUTE && d.solver_status != ECG_SOLVER_CONVERGED_RELATIVE) {
+      out->failed = 1;
+      out->failure_code = ECG_FAILURE_IMEX_SOLVER;
+      break;
+    }
+    out->dt_min = std::min(out->dt_min, dt);
+    out->dt_max = std::max(out->dt_max, dt);
+    out->dt_sum += dt;
+    t += dt;
+    ++steps;
+    e = ecg_compute_diagnostics(c, &dg);
+    if (e != ECG_OK) break;
+    if (dg.nonfinite_count > 0) out->failure_code = ECG_FAILURE_NONFINITE_STATE;
+    else if (dg.rho_min <= 0.0) out->failure_code = ECG_FAILURE_NONPOSITIVE_DENSITY;
+    else if (dg.pressure_min <= 0.0) out->failure_code = ECG_FAILURE_NONPOSITIVE_PRESSURE;
+    out->failed = out->failure_code != 0;
+  }
+  if (!out->failed && steps >= max_step && t < stop_time - 1.0e-14) out->failure_code = ECG_FAILURE_MAX_STEP_BEFORE_STOP_TIME;
+  out->steps = steps;
+  out->time = t;
+  out->diagnostics = dg;
+  c->cfg.stop_time = saved_stop;
+  return e;
 }

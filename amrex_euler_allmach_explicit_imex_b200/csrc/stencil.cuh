@@ -42,6 +42,11 @@ __device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __
     return Cons{__ldg(u + o), __ldg(u + o + pl), __ldg(u + o + 2 * pl), __ldg(u + o + 3 * pl)};
   }
   if (P.bc.ring) {
+    // Tiles and warp strips that overhang the domain load cells past the
+    // two-cell ring; their values feed no in-domain face, so clamp them onto
+    // the ring to keep every read inside it.
+    i = i < -2 ? -2 : (i > nx + 1 ? nx + 1 : i);
+    j = j < -2 ? -2 : (j > ny + 1 ? ny + 1 : j);
     const long long o = static_cast<long long>(j + 2) * P.ring_pitch + (i + 2);
     const long long pl = P.ring_plane;
     return Cons{P.ring[o], P.ring[o + pl], P.ring[o + 2 * pl], P.ring[o + 3 * pl]};
@@ -139,6 +144,66 @@ __device__ __host__ __forceinline__ double euler_dt_from_rate(double max_rate, d
   return (rem < dt) ? rem : dt;
 }
 
+__device__ __forceinline__ void reset_record(EcgStepStats& s)
+{
+  s.max_rate_key = okey(kLowest);
+  s.rho_min_key = okey(kMax);
+  s.p_min_key = okey(kMax);
+  s.nonfinite = 0;
+  s.degenerate = 0;
+  s.t = 0.0;
+  s.dt = 0.0;
+  s.ran = 0;
+  s.halt = 0;
+  s.failure = 0;
+  s.step = 0;
+}
+
+// dt of this launch.  Host mode: ctl.dt.  Device mode: the driver loop's
+// checks and compute_euler_dt on the reductions of the previous launch
+// (driver_main.hpp:224-247, 300-310).  Returns false when the loop stops here
+// (block 0 then records the stop in stats[acc_slot]).
+__device__ __forceinline__ bool step_control(EcgStepStats* __restrict__ stats, const EcgDtCtl& ctl, double& dt)
+{
+  const bool lead = blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0;
+  if (lead && ctl.reset_slot >= 0) reset_record(stats[ctl.reset_slot]);
+  dt = ctl.dt;
+  if (!ctl.device_dt) return true;
+  const EcgStepStats& s = stats[ctl.read_slot];
+  const double t = s.t;
+  int failure = s.halt ? s.failure : 0;
+  bool halt = s.halt != 0;
+  if (!halt) {
+    if (s.nonfinite > 0) failure = ECG_FAILURE_NONFINITE_STATE;
+    else if (okey_inv(s.rho_min_key) <= 0.0) failure = ECG_FAILURE_NONPOSITIVE_DENSITY;
+    else if (okey_inv(s.p_min_key) <= 0.0) failure = ECG_FAILURE_NONPOSITIVE_PRESSURE;
+    halt = failure != 0 || s.step >= ctl.max_step || !(t < ctl.stop_time - 1.0e-14);
+  }
+  if (!halt) {
+    dt = euler_dt_from_rate(okey_inv(s.max_rate_key), ctl.cfl, ctl.stop_time, t);
+    if (!isfinite(dt) || dt <= 0.0) {
+      halt = true;
+      failure = ECG_FAILURE_INVALID_TIME_STEP;
+    }
+  }
+  if (halt) {
+    if (lead) {
+      stats[ctl.acc_slot].halt = 1;
+      stats[ctl.acc_slot].failure = failure;
+      stats[ctl.acc_slot].t = t;
+      stats[ctl.acc_slot].step = s.step;
+    }
+    return false;
+  }
+  if (lead) {
+    stats[ctl.read_slot].dt = dt;
+    stats[ctl.read_slot].ran = 1;
+    stats[ctl.acc_slot].t = t + dt;
+    stats[ctl.acc_slot].step = s.step + 1;
+  }
+  return true;
+}
+
 // ---- the fused explicit step ---------------------------------------------------
 
 template <int TX, int TY, bool XIE>
@@ -197,7 +262,7 @@ __device__ __forceinline__ double face_pressure(const double* sp, int m, int c, 
 template <int RK, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 2)
 fv_step_kernel(const EcgFvParams P, const double* __restrict__ u, double* __restrict__ out,
-               EcgStepStats* __restrict__ stats, const int k, const EcgDtCtl ctl)
+               EcgStepStats* __restrict__ stats, const EcgDtCtl ctl)
 {
   constexpr bool XIE = RK == ECG_RIEMANN_XIE_AM_HLLC_P;
   using S = FvSmem<TX, TY, XIE>;
@@ -216,42 +281,8 @@ fv_step_kernel(const EcgFvParams P, const double* __restrict__ u, double* __rest
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int nx = P.g.nx, ny = P.g.ny;
 
-  // ---- dt and loop control (driver_main.hpp:224-247, 300-310) ----
-  double dt = ctl.dt;
-  if (ctl.device_dt) {
-    const EcgStepStats& s = stats[k];
-    const double t = s.t;
-    int failure = s.halt ? s.failure : 0;
-    bool halt = s.halt != 0;
-    if (!halt) {
-      if (s.nonfinite > 0) failure = ECG_FAILURE_NONFINITE_STATE;
-      else if (okey_inv(s.rho_min_key) <= 0.0) failure = ECG_FAILURE_NONPOSITIVE_DENSITY;
-      else if (okey_inv(s.p_min_key) <= 0.0) failure = ECG_FAILURE_NONPOSITIVE_PRESSURE;
-      halt = failure != 0 || s.step >= ctl.max_step || !(t < ctl.stop_time - 1.0e-14);
-    }
-    if (!halt) {
-      dt = euler_dt_from_rate(okey_inv(s.max_rate_key), ctl.cfl, ctl.stop_time, t);
-      if (!isfinite(dt) || dt <= 0.0) {
-        halt = true;
-        failure = ECG_FAILURE_INVALID_TIME_STEP;
-      }
-    }
-    if (halt) {
-      if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
-        stats[k + 1].halt = 1;
-        stats[k + 1].failure = failure;
-        stats[k + 1].t = t;
-        stats[k + 1].step = s.step;
-      }
-      return;
-    }
-    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
-      stats[k].dt = dt;
-      stats[k].ran = 1;
-      stats[k + 1].t = t + dt;
-      stats[k + 1].step = s.step + 1;
-    }
-  }
+  double dt;
+  if (!step_control(stats, ctl, dt)) return;
 
   // ---- phase A: halo region -> primitives in shared memory ----
   for (int e = tid; e < S::RN; e += NT) {
@@ -391,11 +422,11 @@ fv_step_kernel(const EcgFvParams P, const double* __restrict__ u, double* __rest
     kp = umin64(kp, okey(bad ? -kInf : q.p));
     nonfinite += bad ? 1 : 0;
   }
-  block_commit<NT>(red, kmax, krho, kp, nonfinite, degenerate, &stats[k + 1]);
+  block_commit<NT>(red, kmax, krho, kp, nonfinite, degenerate, &stats[ctl.acc_slot]);
 }
 
 template <int RK, int TY>
-cudaError_t launch_fv_t(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, int k,
+cudaError_t launch_fv_t(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
                         const EcgDtCtl& ctl, cudaStream_t s)
 {
   constexpr int TX = 32, NT = 256;
@@ -404,26 +435,37 @@ cudaError_t launch_fv_t(const EcgFvParams& p, const double* in, double* out, Ecg
   const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::bytes));
   if (e != cudaSuccess) return e;
   const dim3 grid((p.g.nx + TX - 1) / TX, (p.g.ny + TY - 1) / TY);
-  kern<<<grid, NT, S::bytes, s>>>(p, in, out, stats, k, ctl);
+  kern<<<grid, NT, S::bytes, s>>>(p, in, out, stats, ctl);
   return cudaGetLastError();
 }
 
 template <int RK>
-cudaError_t launch_fv_rk(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, int k,
+cudaError_t launch_fv_rk(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
                          const EcgDtCtl& ctl, int tile_y, cudaStream_t s)
 {
-  if (tile_y == 8) return launch_fv_t<RK, 8>(p, in, out, stats, k, ctl, s);
-  return launch_fv_t<RK, 16>(p, in, out, stats, k, ctl, s);
+  if (tile_y == 8) return launch_fv_t<RK, 8>(p, in, out, stats, ctl, s);
+  // 0 (default) in the exact build, 16: the 32x16 tile
+  return launch_fv_t<RK, 16>(p, in, out, stats, ctl, s);
 }
 
-cudaError_t launch_fv_step(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, int k,
+#ifdef ECG_FAST_KERNEL
+#include "fv_fast.cuh"
+#include "fv_march.cuh"
+#endif
+
+cudaError_t launch_fv_step(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
                            const EcgDtCtl& ctl, int tile_y, cudaStream_t s)
 {
+#ifdef ECG_FAST_KERNEL
+  // 0: column-strip marching kernel (default); 1: square-tile kernel
+  if (tile_y == 0) return march::launch(p, in, out, stats, ctl, s);
+  if (tile_y == 1) return fast::launch(p, in, out, stats, ctl, s);
+#endif
   switch (p.riemann) {
-    case ECG_RIEMANN_RUSANOV: return launch_fv_rk<ECG_RIEMANN_RUSANOV>(p, in, out, stats, k, ctl, tile_y, s);
-    case ECG_RIEMANN_LOWMACH_HLLC: return launch_fv_rk<ECG_RIEMANN_LOWMACH_HLLC>(p, in, out, stats, k, ctl, tile_y, s);
-    case ECG_RIEMANN_XIE_AM_HLLC_P: return launch_fv_rk<ECG_RIEMANN_XIE_AM_HLLC_P>(p, in, out, stats, k, ctl, tile_y, s);
-    default: return launch_fv_rk<ECG_RIEMANN_HLLC>(p, in, out, stats, k, ctl, tile_y, s);
+    case ECG_RIEMANN_RUSANOV: return launch_fv_rk<ECG_RIEMANN_RUSANOV>(p, in, out, stats, ctl, tile_y, s);
+    case ECG_RIEMANN_LOWMACH_HLLC: return launch_fv_rk<ECG_RIEMANN_LOWMACH_HLLC>(p, in, out, stats, ctl, tile_y, s);
+    case ECG_RIEMANN_XIE_AM_HLLC_P: return launch_fv_rk<ECG_RIEMANN_XIE_AM_HLLC_P>(p, in, out, stats, ctl, tile_y, s);
+    default: return launch_fv_rk<ECG_RIEMANN_HLLC>(p, in, out, stats, ctl, tile_y, s);
   }
 }
 

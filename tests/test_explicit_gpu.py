@@ -17,12 +17,17 @@ CASES = list(golden_io.explicit_cases())
 FAST_TOL = 1e-12
 
 
-@pytest.mark.parametrize("arith", ["exact", "fast"])
+# (arith, explicit kernel): exact tile kernel; fast column-strip kernel
+# (default); fast square-tile kernel
+KERNELS = [("exact", 0), ("fast", 0), ("fast", 1)]
+
+
+@pytest.mark.parametrize("arith,kernel", KERNELS, ids=["exact", "fast-strip", "fast-tile"])
 @pytest.mark.parametrize("key,case", CASES, ids=[k for k, _ in CASES])
-def test_explicit_step_parity(gpu, arith, key, case):
+def test_explicit_step_parity(gpu, arith, kernel, key, case):
     cfg = read_config(golden_io.kv_of(case["kv"])).cfg
     t, dt = float(case["t"]), float(case["dt"])
-    with api.Context(cfg, arith=arith) as ctx:
+    with api.Context(cfg, arith=arith, tile_y=kernel) as ctx:
         ctx.upload(case["u0"])
         g = api.fill_problem_ghosts(ctx, t)
         deg = api.euler_fv_one_step(ctx, dt, t)
@@ -122,7 +127,7 @@ def _smooth_periodic(nx, ny, rng):
     return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)])
 
 
-@pytest.mark.parametrize("riemann", ["hllc", "xie_am_hllc_p"])
+@pytest.mark.parametrize("riemann", ["hllc", "xie_am_hllc_p", "rusanov", "lowmach_hllc"])
 def test_full_size_properties(gpu, riemann):
     """2560x640 (the benchmark size): fast vs exact arithmetic within 1e-12
     per step, and periodic mass/momentum/energy conservation to rounding."""
