@@ -146,6 +146,7 @@ EcgFvParams fv_params(ecg_ctx* c, bool imex_policy)
   p.order = c->cfg.spatial_order;
   p.limiter = c->cfg.slope_limiter;
   p.riemann = c->cfg.riemann;
+  p.march_rows = c->opt.tile_x;
   return p;
 }
 

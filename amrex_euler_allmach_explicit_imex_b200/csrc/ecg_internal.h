@@ -53,7 +53,7 @@ struct EcgFvParams {
   long long ring_pitch, ring_plane;
   double gamma;
   int order, limiter, riemann;
-  int pad;
+  int march_rows;            // rows per warp of the column-strip kernel (8, 16, 32, 64; 0: default)
 };
 
 // Per-step reduction record.  Keys are order-preserving integer images of

@@ -73,7 +73,7 @@ __device__ __forceinline__ Cons to_cons_f(const Prim& q, double inv_gm1)
   return Cons{q.rho, q.rho * q.u, q.rho * q.v, fma(q.p, inv_gm1, kin)};
 }
 
-static __device__ __noinline__ Cons rusanov_f(const Prim& l, const Prim& r, int axis, double g, double inv_gm1)
+__device__ __forceinline__ Cons rusanov_i(const Prim& l, const Prim& r, int axis, double g, double inv_gm1)
 {
   const Cons ul = to_cons_f(l, inv_gm1), ur = to_cons_f(r, inv_gm1);
   const Cons fl = pflux(l, ul, axis), fr = pflux(r, ur, axis);
@@ -84,6 +84,13 @@ static __device__ __noinline__ Cons rusanov_f(const Prim& l, const Prim& r, int 
               0.5 * (fl.my + fr.my) - hs * (ur.my - ul.my), 0.5 * (fl.E + fr.E) - hs * (ur.E - ul.E)};
 }
 
+// Out-of-line copy for the rarely taken fallbacks; arguments by value so
+// they travel in registers rather than through the stack.
+static __device__ __noinline__ Cons rusanov_f(Prim l, Prim r, int axis, double g, double inv_gm1)
+{
+  return rusanov_i(l, r, axis, g, inv_gm1);
+}
+
 // hllc_flux (reconstruction_fluxes.hpp:151-210), fast arithmetic.  deg: the
 // star-state degeneracy test (:117-149) of these states.
 __device__ __forceinline__ Cons hllc_f(const Prim& l, const Prim& r, int axis, double g, double inv_gm1, bool& deg)
@@ -91,40 +98,39 @@ __device__ __forceinline__ Cons hllc_f(const Prim& l, const Prim& r, int axis, d
   const double unl = normal_vel(l, axis), unr = normal_vel(r, axis);
   const double cl = fsound(l.rho, l.p, g), cr = fsound(r.rho, r.p, g);
   const double sl = smin(unl - cl, unr - cr), sr = smax(unl + cl, unr + cr);
-  deg = false;
-  if (!(sl < sr)) {
-    deg = true;
-    return rusanov_f(l, r, axis, g, inv_gm1);
+  deg = true;
+  // The three degenerate exits share one inline Rusanov evaluation at the end.
+  if (sl < sr) {
+    if (sl >= 0.0 || sr <= 0.0) {
+      deg = false;
+      const Prim& q = sl >= 0.0 ? l : r;
+      return pflux(q, to_cons_f(q, inv_gm1), axis);
+    }
+    const double al = l.rho * (sl - unl), ar = r.rho * (sr - unr);
+    const double den = al - ar;
+    if (!(fabs(den) <= 1.0e-12)) {
+      const double sm = fdiv(r.p - l.p + al * unl - ar * unr, den);
+      const double lsd = sl - sm, rsd = sr - sm;
+      if (!(fabs(lsd) <= 1.0e-12 || fabs(rsd) <= 1.0e-12)) {
+        deg = false;
+        const double ps = 0.5 * (l.p + al * (sm - unl) + r.p + ar * (sm - unr));
+        const bool left = sm >= 0.0;
+        const Prim q = left ? l : r;
+        const double s = left ? sl : sr, un = left ? unl : unr, a = left ? al : ar;
+        const double inv_sd = frcp(left ? lsd : rsd);
+        const Cons u = to_cons_f(q, inv_gm1);
+        const Cons f = pflux(q, u, axis);
+        const double rs = a * inv_sd;
+        const double es = ((s - un) * u.E - q.p * un + ps * sm) * inv_sd;
+        const double tang = axis == 0 ? q.v : q.u;
+        const double smx = axis == 0 ? rs * sm : rs * tang;
+        const double smy = axis == 0 ? rs * tang : rs * sm;
+        return Cons{fma(s, rs - u.rho, f.rho), fma(s, smx - u.mx, f.mx), fma(s, smy - u.my, f.my),
+                    fma(s, es - u.E, f.E)};
+      }
+    }
   }
-  if (sl >= 0.0 || sr <= 0.0) {
-    const Prim& q = sl >= 0.0 ? l : r;
-    return pflux(q, to_cons_f(q, inv_gm1), axis);
-  }
-  const double al = l.rho * (sl - unl), ar = r.rho * (sr - unr);
-  const double den = al - ar;
-  if (fabs(den) <= 1.0e-12) {
-    deg = true;
-    return rusanov_f(l, r, axis, g, inv_gm1);
-  }
-  const double sm = fdiv(r.p - l.p + al * unl - ar * unr, den);
-  const double lsd = sl - sm, rsd = sr - sm;
-  if (fabs(lsd) <= 1.0e-12 || fabs(rsd) <= 1.0e-12) {
-    deg = true;
-    return rusanov_f(l, r, axis, g, inv_gm1);
-  }
-  const double ps = 0.5 * (l.p + al * (sm - unl) + r.p + ar * (sm - unr));
-  const bool left = sm >= 0.0;
-  const Prim q = left ? l : r;
-  const double s = left ? sl : sr, un = left ? unl : unr, a = left ? al : ar;
-  const double inv_sd = frcp(left ? lsd : rsd);
-  const Cons u = to_cons_f(q, inv_gm1);
-  const Cons f = pflux(q, u, axis);
-  const double rs = a * inv_sd;
-  const double es = ((s - un) * u.E - q.p * un + ps * sm) * inv_sd;
-  const double tang = axis == 0 ? q.v : q.u;
-  const double smx = axis == 0 ? rs * sm : rs * tang;
-  const double smy = axis == 0 ? rs * tang : rs * sm;
-  return Cons{fma(s, rs - u.rho, f.rho), fma(s, smx - u.mx, f.mx), fma(s, smy - u.my, f.my), fma(s, es - u.E, f.E)};
+  return rusanov_i(l, r, axis, g, inv_gm1);
 }
 
 // low_mach_correct_velocity_states (reconstruction_fluxes.hpp:212-232), fast arithmetic.
@@ -145,7 +151,7 @@ __device__ __forceinline__ void lowmach_f(Prim& l, Prim& r, double g)
 }
 
 // xie_am_hllc_p_flux (reconstruction_fluxes.hpp:254-371), fast arithmetic.
-static __device__ __noinline__ Cons xie_f(const Prim& l, const Prim& r, int axis, double g, double inv_gm1,
+static __device__ __noinline__ Cons xie_f(const Prim l, const Prim r, int axis, double g, double inv_gm1,
                                           double sensor, bool& deg)
 {
   const double ql = normal_vel(l, axis), qr = normal_vel(r, axis);

@@ -46,7 +46,7 @@ template <int RK>
 __device__ __forceinline__ Cons riemann(Prim L, Prim R, int axis, double g, double inv_gm1, bool& deg)
 {
   deg = false;
-  if (RK == ECG_RIEMANN_RUSANOV) return fast::rusanov_f(L, R, axis, g, inv_gm1);
+  if (RK == ECG_RIEMANN_RUSANOV) return fast::rusanov_i(L, R, axis, g, inv_gm1);
   if (RK == ECG_RIEMANN_LOWMACH_HLLC) fast::lowmach_f(L, R, g);
   return fast::hllc_f(L, R, axis, g, inv_gm1, deg);
 }
@@ -148,15 +148,27 @@ fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __res
   block_commit<WPB * 32>(red, kmax, krho, kp, nonfinite, degenerate, &stats[ctl.acc_slot]);
 }
 
-template <int RK>
-cudaError_t launch_rk(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
-                      cudaStream_t s)
+template <int RK, int H>
+cudaError_t launch_h(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
+                     cudaStream_t s)
 {
-  constexpr int H = 32, WPB = 4;
+  constexpr int WPB = 4;
   const int strips = (p.g.nx + kCells - 1) / kCells;
   const dim3 grid((strips + WPB - 1) / WPB, (p.g.ny + H - 1) / H);
   fv_march_kernel<RK, H, WPB><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl);
   return cudaGetLastError();
+}
+
+template <int RK>
+cudaError_t launch_rk(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
+                      cudaStream_t s)
+{
+  switch (p.march_rows) {
+    case 8: return launch_h<RK, 8>(p, in, out, stats, ctl, s);
+    case 16: return launch_h<RK, 16>(p, in, out, stats, ctl, s);
+    case 64: return launch_h<RK, 64>(p, in, out, stats, ctl, s);
+    default: return launch_h<RK, 32>(p, in, out, stats, ctl, s);
+  }
 }
 
 inline cudaError_t launch(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
