@@ -42,6 +42,8 @@ SIGNATURES = {
     "ecg_run": (C.c_int, [_CTX, _I32, _D, C.POINTER(abi.RunResult)]),
     "ecg_explicit_step_vjp_device": (C.c_int, [_CTX, _P, _D, _P, _P]),
     "ecg_explicit_step_device": (C.c_int, [_CTX, _P, _D, _P]),
+    "ecg_euler_fv_one_step_noalloc": (C.c_int, [C.POINTER(abi.RunConfig), C.POINTER(abi.GpuOptions), _P, _P, _I32,
+                                                _I32, _I64, _I64, _D, _D, C.POINTER(_I32), C.c_char_p, _I32]),
     "ecg_batch_create": (C.c_int, [C.POINTER(_P), _I32, C.POINTER(abi.RunConfig), C.POINTER(abi.GpuOptions)]),
     "ecg_batch_destroy": (None, [_P]),
     "ecg_batch_upload": (C.c_int, [_P, _I32, _P, _I32, _I32, _I64, _I64]),

@@ -36,6 +36,7 @@ SOURCES = {
     "imex.cu": [],
     "batched.cu": ["-fmad=true"],
     "adjoint.cu": ["-fmad=true"],
+    "noalloc.cu": [],
 }
 
 

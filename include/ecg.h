@@ -348,6 +348,29 @@ ecg_status ecg_explicit_step_vjp_device(ecg_ctx* ctx, const double* u0, double d
  * checkpointed adjoint: u1 = euler_fv_one_step(u0; dt). */
 ecg_status ecg_explicit_step_device(ecg_ctx* ctx, const double* u0, double dt, double* u1);
 
+/* ---- allocation-free explicit step -------------------------------------- */
+/* No counterpart in the reference: euler_fv_one_step
+ * (numerics/explicit_update.hpp:58-102) on caller-owned DEVICE arrays with no
+ * context and no device or host allocation, for callers that cannot allocate
+ * inside their time loop (an AMReX GPU build whose arena reserves most of HBM
+ * at start-up and whose stream pipeline a cudaFree would synchronise).
+ * state_in/state_out: distinct device arrays in the Array4 layout of
+ * ecg_upload_state (same lo, jstride, nstride for both); ghost cells come from
+ * the boundary conditions of cfg.  opt may be NULL (defaults; opt->stream is
+ * the stream the work is queued on, opt->device the device).  Scratch lives
+ * in one static device array of ECG_NOALLOC_SCRATCH_BYTES per device: the
+ * exact-Dirichlet problems need 32*(nx+4)*(ny+4) bytes of it for their ghost
+ * ring and are rejected with ECG_ERR_BAD_ARG beyond that; the others have no
+ * size limit.  Calls that overlap in time on one device race on that scratch.
+ * The first call on a device looks the scratch up (make it before any stream
+ * capture).  hllc_degenerate_count (may be NULL) synchronises the stream.  On
+ * failure a message is written to err (err_len bytes, may be NULL). */
+#define ECG_NOALLOC_SCRATCH_BYTES (8u << 20)
+ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gpu_options* opt,
+                                         const double* state_in, double* state_out, int32_t lo_x, int32_t lo_y,
+                                         int64_t jstride, int64_t nstride, double dt, double time,
+                                         int32_t* hllc_degenerate_count, char* err, int32_t err_len);
+
 /* ---- batched independent solves ----------------------------------------- */
 /* Many explicit O2 solves of uneven grid sizes advanced together by one
  * persistent launch per step (captured in a CUDA graph).  Each solve keeps

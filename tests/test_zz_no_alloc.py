@@ -1,0 +1,126 @@
+"""The allocation-free explicit step, ecg_euler_fv_one_step_noalloc, against
+the context entry point ecg_euler_fv_one_step on the same inputs.
+
+Both are called through the C ABI.  The caller's state lives in an AMReX-style
+FArrayBox with two ghost cells (lo = (-2, -2)); two calls in a row
+(in -> out, then out -> in) must reproduce two context steps: bit-identical in
+ECG_ARITH_EXACT, within 1e-12 relative per step in ECG_ARITH_FAST.  The file
+name sorts last so the suite also runs it after every other GPU test."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from amrex_euler_allmach_explicit_imex_b200 import _lib, api
+from amrex_euler_allmach_explicit_imex_b200.config import read_config
+from tests import golden_io
+
+pytestmark = pytest.mark.gpu
+
+FAST_TOL = 1e-12
+CASES = list(golden_io.explicit_cases())
+
+
+def _noalloc(cfg, opt, src, dst, nx, ny, dt, t):
+    lib = _lib.load()
+    err = C.create_string_buffer(512)
+    deg = C.c_int32(-1)
+    # Array4 base = the box's lower corner (-2, -2)
+    st = lib.ecg_euler_fv_one_step_noalloc(C.byref(cfg), C.byref(opt), C.c_void_p(src.data_ptr()),
+                                           C.c_void_p(dst.data_ptr()), -2, -2, nx + 4, (nx + 4) * (ny + 4), dt, t,
+                                           C.byref(deg), err, len(err))
+    return st, deg.value, err.value.decode()
+
+
+def _fab(torch, u):
+    """(4, ny, nx) valid data -> device FArrayBox (4, ny+4, nx+4) with NaN ghosts."""
+    _, ny, nx = u.shape
+    f = torch.full((4, ny + 4, nx + 4), float("nan"), dtype=torch.float64, device="cuda")
+    f[:, 2:ny + 2, 2:nx + 2] = torch.from_numpy(np.ascontiguousarray(u)).cuda()
+    return f
+
+
+def _check(arith, got, want):
+    if arith == "exact":
+        assert np.array_equal(got, want)
+    else:
+        assert golden_io.state_rel_err(got, want) <= FAST_TOL
+
+
+def _two_steps(cfg, u0, dt, t, arith):
+    import torch
+
+    nx, ny = cfg.n_cell[0], cfg.n_cell[1]
+    with api.Context(cfg, arith=arith) as ctx:
+        ctx.upload(u0)
+        deg1 = api.euler_fv_one_step(ctx, dt, t)
+        u1 = ctx.download()
+        deg2 = api.euler_fv_one_step(ctx, dt, t + dt)
+        u2 = ctx.download()
+
+    a = _fab(torch, u0)
+    b = torch.full_like(a, float("nan"))
+    opt = api.gpu_options(arith=arith, stream=torch.cuda.current_stream().cuda_stream)
+    st, d1, msg = _noalloc(cfg, opt, a, b, nx, ny, dt, t)
+    assert st == 0, msg
+    torch.cuda.synchronize()
+    _check(arith, b[:, 2:ny + 2, 2:nx + 2].cpu().numpy(), u1)
+    assert d1 == deg1
+    st, d2, msg = _noalloc(cfg, opt, b, a, nx, ny, dt, t + dt)
+    assert st == 0, msg
+    torch.cuda.synchronize()
+    _check(arith, a[:, 2:ny + 2, 2:nx + 2].cpu().numpy(), u2)
+    assert d2 == deg2
+    # the caller's ghost cells are never written
+    assert torch.isnan(a[:, :2]).all() and torch.isnan(b[:, :, -2:]).all()
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+@pytest.mark.parametrize("key,case", CASES, ids=[k for k, _ in CASES])
+def test_noalloc_matches_context_step(gpu, arith, key, case):
+    cfg = read_config(golden_io.kv_of(case["kv"])).cfg
+    _two_steps(cfg, case["u0"], float(case["dt"]), float(case["t"]), arith)
+
+
+def _random_state(nx, ny, seed):
+    rng = np.random.default_rng(seed)
+    rho = rng.uniform(1.0, 2.0, (ny, nx))
+    u = rng.uniform(-0.5, 0.5, (ny, nx))
+    v = rng.uniform(-0.5, 0.5, (ny, nx))
+    p = rng.uniform(1.0, 2.0, (ny, nx))
+    return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)])
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+@pytest.mark.parametrize("problem,riemann", [("gresho_vortex", "hllc"), ("toro1", "xie_am_hllc_p"),
+                                             ("shock_density_bubble_2d", "hllc"), ("advection_blob", "lowmach_hllc")])
+def test_noalloc_larger_grid(gpu, arith, problem, riemann):
+    """A 200 x 120 grid: strips and tiles that overhang the domain, the
+    exact-Dirichlet ghost ring in the static scratch."""
+    hi = "2 0.5" if problem.startswith("shock") else "1 0.6"
+    kv = (f"amr.n_cell=200 120\neuler.problem={problem}\neuler.riemann={riemann}\n"
+          "euler.spatial_order=2\neuler.field_boundary=exact_dirichlet\ngeometry.is_periodic=0 0\n"
+          f"geometry.prob_hi={hi}\n")
+    cfg = read_config(kv).cfg
+    _two_steps(cfg, _random_state(200, 120, 5), 2.0e-4, 0.01, arith)
+
+
+def test_noalloc_rejects_ring_beyond_scratch(gpu):
+    import torch
+
+    kv = "amr.n_cell=2048 300\neuler.problem=toro1\neuler.field_boundary=exact_dirichlet\ngeometry.is_periodic=0 0\n"
+    cfg = read_config(kv).cfg
+    a = torch.zeros(16, dtype=torch.float64, device="cuda")
+    b = torch.zeros(16, dtype=torch.float64, device="cuda")
+    opt = api.gpu_options()
+    lib = _lib.load()
+    err = C.create_string_buffer(512)
+    st = lib.ecg_euler_fv_one_step_noalloc(C.byref(cfg), C.byref(opt), C.c_void_p(a.data_ptr()),
+                                           C.c_void_p(b.data_ptr()), 0, 0, 2048, 2048 * 300, 1e-4, 0.0, None, err,
+                                           len(err))
+    assert st == 1  # ECG_ERR_BAD_ARG, before any launch
+    assert "exceeds" in err.value.decode()
+    st = lib.ecg_euler_fv_one_step_noalloc(C.byref(cfg), C.byref(opt), C.c_void_p(a.data_ptr()),
+                                           C.c_void_p(a.data_ptr()), 0, 0, 2048, 2048 * 300, 1e-4, 0.0, None, err,
+                                           len(err))
+    assert st == 1
