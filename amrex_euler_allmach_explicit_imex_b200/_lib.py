@@ -33,6 +33,7 @@ SIGNATURES = {
     "ecg_download_state_device": (C.c_int, [_CTX, _P, _I32, _I32, _I64, _I64]),
     "ecg_fill_problem_ghosts": (C.c_int, [_CTX, _D, _P]),
     "ecg_synchronize": (C.c_int, [_CTX]),
+    "ecg_initialize_state": (C.c_int, [_CTX]),
     "ecg_euler_fv_one_step": (C.c_int, [_CTX, _D, _D, C.POINTER(_I32)]),
     "ecg_compute_euler_dt": (C.c_int, [_CTX, _D, C.POINTER(_D)]),
     "ecg_compute_imex_dt": (C.c_int, [_CTX, _D, C.POINTER(_D), C.POINTER(abi.ImexTimestepDiag)]),

@@ -111,6 +111,11 @@ class Context:
         check(load().ecg_synchronize(self._h), "synchronize", self._h)
 
 
+def initialize_state(ctx):
+    """initialize_state (problems/problem_initialization.hpp:420-435) on the device."""
+    check(load().ecg_initialize_state(ctx.handle), "initialize_state", ctx.handle)
+
+
 def euler_fv_one_step(ctx, dt, time=0.0):
     """One explicit step; returns the HLLC degenerate-star count."""
     n = C.c_int32()
@@ -170,7 +175,69 @@ def run(ctx, max_step, stop_time):
     return r
 
 
+class Batch:
+    """Many independent explicit solves of uneven grid sizes advanced together
+    (ecg_batch_*): one persistent launch per step for the whole batch, CUDA
+    graphs of 24 steps, dt per solve on the device."""
+
+    def __init__(self, cfgs, **gpu):
+        lib = load()
+        cfgs = [c.cfg if isinstance(c, RunSettings) else (c if isinstance(c, abi.RunConfig) else read_config(c).cfg)
+                for c in cfgs]
+        self.n = len(cfgs)
+        self.cfgs = (abi.RunConfig * self.n)(*[c.copy() for c in cfgs])
+        self.opt = gpu_options(**gpu)
+        h = C.c_void_p()
+        code = lib.ecg_batch_create(C.byref(h), self.n, self.cfgs, C.byref(self.opt))
+        if code != 0:
+            raise EcgError(code, "ecg_batch_create: " + lib.ecg_status_str(code).decode())
+        self._h = h
+        self.shapes = [(c.n_cell[1], c.n_cell[0]) for c in cfgs]
+
+    def _check(self, code, what):
+        if code != 0:
+            lib = load()
+            raise EcgError(code, f"{what}: {lib.ecg_status_str(code).decode()}: {lib.ecg_batch_last_error(self._h).decode()}")
+
+    def upload(self, k, u):
+        ny, nx = self.shapes[k]
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.shape != (4, ny, nx):
+            raise ValueError(f"state shape {u.shape} != (4, {ny}, {nx})")
+        self._check(load().ecg_batch_upload(self._h, k, u.ctypes.data, 0, 0, nx, nx * ny), "batch upload")
+
+    def download(self, k):
+        ny, nx = self.shapes[k]
+        out = np.empty((4, ny, nx), dtype=np.float64)
+        self._check(load().ecg_batch_download(self._h, k, out.ctypes.data, 0, 0, nx, nx * ny), "batch download")
+        return out
+
+    def run(self, steps):
+        """Advances every solve by up to `steps` steps; returns one BatchResult per solve."""
+        res = (abi.BatchResult * self.n)()
+        self._check(load().ecg_batch_run(self._h, steps, res), "batch run")
+        return list(res)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().ecg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 __all__ = [
+    "Batch",
     "Context",
     "EcgError",
     "compute_admissibility_diagnostics",
@@ -181,6 +248,7 @@ __all__ = [
     "euler_imex_bdltv20_o1_source_map_picard_one_step",
     "fill_problem_ghosts",
     "gpu_options",
+    "initialize_state",
     "read_config",
     "run",
     "solver_status_str",

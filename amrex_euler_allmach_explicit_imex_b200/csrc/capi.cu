@@ -225,6 +225,8 @@ ecg_ctx::~ecg_ctx()
   cudaFree(d_ring);
   cudaFree(d_stats);
   cudaFree(d_state_stats);
+  cudaFree(adj_gq);
+  cudaFree(adj_stats);
   cudaFreeHost(h_stats);
   cudaFreeHost(h_state_stats);
   if (own_stream && stream) cudaStreamDestroy(stream);
@@ -460,6 +462,17 @@ ecg_status ecg_download_state_device(ecg_ctx* c, double* base, int32_t lo_x, int
 {
   if (c && !c->uploaded) return ECG_ERR_NOT_READY;
   return transfer(c, base, nullptr, lo_x, lo_y, jstride, nstride, false, true);
+}
+
+ecg_status ecg_initialize_state(ecg_ctx* c)
+{
+  if (!c) return ECG_ERR_BAD_ARG;
+  const EcgFvParams p = fv_params(c, false);
+  const EcgProblem pr = problem_of(c, false);
+  if (!cuda_ok(c, c->ops->init_state(p, pr, c->cur_state_mut(), c->stream), "initialize state")) return ECG_ERR_CUDA;
+  c->uploaded = true;
+  c->invalidate();
+  return ECG_OK;
 }
 
 ecg_status ecg_fill_problem_ghosts(ecg_ctx* c, double time, double* ghosted_host)

@@ -56,6 +56,9 @@ struct ecg_ctx {
   std::vector<Graph> graphs;
 
   EcgImexState* imex = nullptr;
+  // adjoint workspace (adjoint.cu): primitive gradients, one stats record
+  double* adj_gq = nullptr;
+  EcgStepStats* adj_stats = nullptr;
   std::string err;
 
   const double* cur_state() const { return d_state[cur]; }

@@ -84,6 +84,25 @@ struct EcgDtCtl {
   double cfl, stop_time;
 };
 
+// One solve of a batch (batched.cu).  u[k & 1] holds the state after k
+// steps of this solve.
+struct EcgBatchSolve {
+  EcgFvParams p;         // grid, boundary policy and physics of the solve
+  double* u[2];          // state double buffer (pitch p.g.pitch, plane p.g.plane)
+  double cfl, stop_time;
+  int tile0;             // first tile of this solve in the batch's tile list
+  int strip_blocks;      // tiles across x
+  int row_blocks;        // tiles along y
+  int pad;
+};
+
+// Per-launch control of a batched step.
+struct EcgBatchCtl {
+  int nsolve, ntiles;
+  int read_slot, acc_slot, reset_slot;  // rotation over each solve's three records
+  int count_degenerate;
+};
+
 // Whole-state reductions (one pass).
 struct EcgStateStats {
   unsigned long long max_rate_key;        // compute_euler_dt
@@ -110,7 +129,20 @@ struct EcgStencilOps {
   cudaError_t (*init_stats)(EcgStepStats* stats, int n, double t0, cudaStream_t s);
   cudaError_t (*init_state_stats)(EcgStateStats* st, cudaStream_t s);
   cudaError_t (*seed_stats)(EcgStepStats* stats, const EcgStateStats* st, cudaStream_t s);
+  cudaError_t (*init_state)(const EcgFvParams& p, const EcgProblem& pr, double* u, cudaStream_t s);
 };
+
+namespace ecg_fast {
+// Batched step launcher and tile geometry (fv_batch.cuh, fast build).
+cudaError_t launch_batch_step(int riemann, int limiter, int shape, const EcgBatchSolve* solves, EcgStepStats* stats,
+                              unsigned long long* degenerate_total, const int* max_step, const EcgBatchCtl& ctl,
+                              int grid, cudaStream_t st);
+void batch_tiles(int nx, int ny, int shape, int& strip_blocks, int& row_blocks);
+int batch_block_threads(int shape);
+int batch_blocks_per_sm(int riemann, int limiter, int shape);
+cudaError_t launch_batch_rearm(EcgStepStats* stats, int nsolve, int read_slot, cudaStream_t st);
+constexpr int kBatchShapes = 3;
+}  // namespace ecg_fast
 
 extern const EcgStencilOps ecg_exact_ops;
 extern const EcgStencilOps ecg_fast_ops;

@@ -133,6 +133,70 @@ __device__ __forceinline__ Cons hllc_f(const Prim& l, const Prim& r, int axis, d
   return rusanov_i(l, r, axis, g, inv_gm1);
 }
 
+// 0 < x < 1e300 by one unsigned integer compare of the bit pattern (positive
+// doubles order like their bits; zero, negatives, NaN and huge values fail).
+__device__ __forceinline__ bool pos_normal_range(double x)
+{
+  constexpr unsigned long long kHi = 0x7E37E43C8800759CULL;  // bits of 1.0e300
+  return static_cast<unsigned long long>(__double_as_longlong(x)) - 1ULL < kHi - 1ULL;
+}
+
+// fsound for whole warps: the rsqrt path, and the IEEE formula only when some
+// lane of the warp has a state outside (0, 1e300) (a uniform branch).
+__device__ __forceinline__ double fsound_w(double rho, double p, double g)
+{
+  const double t = g * p;
+  const double q = t * rho;
+  double c = t * frsqrt(q);
+  const bool ok = pos_normal_range(q);
+  if (__any_sync(0xffffffffu, !ok)) {
+    if (!ok) c = sqrt(t / rho);
+  }
+  return c;
+}
+
+// hllc_flux of hllc_f without divergent branches: every lane evaluates the
+// star-state flux of its upwind side, supersonic faces select the plain
+// physical flux, and the Rusanov fallback (the three degenerate cases of
+// reconstruction_fluxes.hpp:151-210) runs only when some lane of the warp
+// needs it.  deg: that fallback was taken.
+__device__ __forceinline__ Cons hllc_w(const Prim& l, const Prim& r, int axis, double g, double inv_gm1, bool& deg)
+{
+  const double unl = normal_vel(l, axis), unr = normal_vel(r, axis);
+  const double cl = fsound_w(l.rho, l.p, g), cr = fsound_w(r.rho, r.p, g);
+  const double sl = smin(unl - cl, unr - cr), sr = smax(unl + cl, unr + cr);
+  const bool ordered = sl < sr;
+  const bool sup_l = sl >= 0.0, sup_r = sr <= 0.0;
+  const bool supersonic = ordered && (sup_l || sup_r);
+  const double al = l.rho * (sl - unl), ar = r.rho * (sr - unr);
+  const double den = al - ar;
+  const double sm = fdiv(r.p - l.p + al * unl - ar * unr, den);
+  const double lsd = sl - sm, rsd = sr - sm;
+  deg = !ordered || (!supersonic && (fabs(den) <= 1.0e-12 || fabs(lsd) <= 1.0e-12 || fabs(rsd) <= 1.0e-12));
+  const bool left = supersonic ? sup_l : sm >= 0.0;
+  const Prim q = left ? l : r;
+  const double s = left ? sl : sr, un = left ? unl : unr, a = left ? al : ar;
+  const Cons u = to_cons_f(q, inv_gm1);
+  const Cons f = pflux(q, u, axis);
+  const double ps = 0.5 * (l.p + al * (sm - unl) + r.p + ar * (sm - unr));
+  const double inv_sd = frcp(left ? lsd : rsd);
+  const double rs = a * inv_sd;
+  const double es = ((s - un) * u.E - q.p * un + ps * sm) * inv_sd;
+  const double tang = axis == 0 ? q.v : q.u;
+  const double smx = axis == 0 ? rs * sm : rs * tang;
+  const double smy = axis == 0 ? rs * tang : rs * sm;
+  Cons out;
+  out.rho = supersonic ? f.rho : fma(s, rs - u.rho, f.rho);
+  out.mx = supersonic ? f.mx : fma(s, smx - u.mx, f.mx);
+  out.my = supersonic ? f.my : fma(s, smy - u.my, f.my);
+  out.E = supersonic ? f.E : fma(s, es - u.E, f.E);
+  if (__any_sync(0xffffffffu, deg)) {
+    const Cons rf = rusanov_i(l, r, axis, g, inv_gm1);
+    if (deg) out = rf;
+  }
+  return out;
+}
+
 // low_mach_correct_velocity_states (reconstruction_fluxes.hpp:212-232), fast arithmetic.
 __device__ __forceinline__ void lowmach_f(Prim& l, Prim& r, double g)
 {

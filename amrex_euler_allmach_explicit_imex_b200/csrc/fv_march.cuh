@@ -26,11 +26,12 @@ struct Lane {
 __device__ __forceinline__ double shup(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 __device__ __forceinline__ double shdn(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
-__device__ __forceinline__ Prim slope3(const Prim& m, const Prim& c, const Prim& p, int lim, bool second)
+template <int LIM>
+__device__ __forceinline__ Prim slope3(const Prim& m, const Prim& c, const Prim& p, bool second)
 {
   if (!second) return Prim{0.0, 0.0, 0.0, 0.0};
-  return Prim{limited_slope(c.rho - m.rho, p.rho - c.rho, lim), limited_slope(c.u - m.u, p.u - c.u, lim),
-              limited_slope(c.v - m.v, p.v - c.v, lim), limited_slope(c.p - m.p, p.p - c.p, lim)};
+  return Prim{limited_slope(c.rho - m.rho, p.rho - c.rho, LIM), limited_slope(c.u - m.u, p.u - c.u, LIM),
+              limited_slope(c.v - m.v, p.v - c.v, LIM), limited_slope(c.p - m.p, p.p - c.p, LIM)};
 }
 
 __device__ __forceinline__ Prim plus_half(const Prim& q, const Prim& s)
@@ -48,126 +49,159 @@ __device__ __forceinline__ Cons riemann(Prim L, Prim R, int axis, double g, doub
   deg = false;
   if (RK == ECG_RIEMANN_RUSANOV) return fast::rusanov_i(L, R, axis, g, inv_gm1);
   if (RK == ECG_RIEMANN_LOWMACH_HLLC) fast::lowmach_f(L, R, g);
-  return fast::hllc_f(L, R, axis, g, inv_gm1, deg);
+  return fast::hllc_w(L, R, axis, g, inv_gm1, deg);
 }
 
-template <int RK, int H, int WPB>
+// Reductions of one warp strip over the new state.
+struct MarchAcc {
+  unsigned long long kmax, krho, kp;
+  int nonfinite, degenerate;
+  __device__ __forceinline__ void init()
+  {
+    kmax = okey(kLowest);
+    krho = okey(kMax);
+    kp = okey(kMax);
+    nonfinite = degenerate = 0;
+  }
+};
+
+// Advances the strip of 28 cells starting at column c0 over rows
+// [j0, min(j0 + H, ny)) from u into out.  Called by all 32 lanes of a warp
+// (the flux helpers vote across the warp).
+template <int RK, int LIM, int H>
+__device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* __restrict__ u,
+                                            double* __restrict__ out, int c0, int j0, double dt, bool count_deg,
+                                            MarchAcc& acc)
+{
+  const int lane = threadIdx.x & 31;
+  const int x = c0 - 2 + lane;
+  const int nx = P.g.nx, ny = P.g.ny;
+  const double g = P.gamma, inv_gm1 = fast::frcp(g - 1.0);
+  const double idx = P.g.inv_dx, idy = P.g.inv_dy;
+  const bool second = P.order > 1;
+  const bool inner = lane >= 2 && lane < 2 + kCells;   // owns a cell of the strip
+  const bool cell_ok = inner && x < nx;                 // that cell is in the domain
+  const bool xface = lane >= 2 && lane <= 2 + kCells;   // its x-face on the left belongs to the strip
+  const int xs = x < 0 ? 0 : (x < nx ? x : nx - 1);     // in-bounds column for the old-state reload
+  const int jend = j0 + H < ny ? j0 + H : ny;
+
+  // ---- prologue: rows j0-2 .. j0+1, y-slopes of rows j0-1 and j0, the y-face below row j0 ----
+  Prim q_m2 = fast::to_prim_f(load_cell(P, u, x, j0 - 2), g);
+  Lane L;
+  L.q[1] = fast::to_prim_f(load_cell(P, u, x, j0 - 1), g);
+  L.q[2] = fast::to_prim_f(load_cell(P, u, x, j0), g);
+  L.q[3] = fast::to_prim_f(load_cell(P, u, x, j0 + 1), g);
+  const Prim sy_m1 = slope3<LIM>(q_m2, L.q[1], L.q[2], second);
+  Prim sy_cur = slope3<LIM>(L.q[1], L.q[2], L.q[3], second);
+  Cons gb;
+  {
+    bool deg;
+    gb = riemann<RK>(plus_half(L.q[1], sy_m1), minus_half(L.q[2], sy_cur), 1, g, inv_gm1, deg);
+    if (count_deg && deg && cell_ok && j0 < ny) acc.degenerate += 1;
+  }
+  for (int j = j0; j < jend; ++j) {
+    // window rows j-1 .. j+2
+    L.q[0] = L.q[1];
+    L.q[1] = L.q[2];
+    L.q[2] = L.q[3];
+    L.q[3] = fast::to_prim_f(load_cell(P, u, x, j + 2), g);
+    const Prim& qc = L.q[1];
+    // y-face above row j
+    const Prim sy_next = slope3<LIM>(L.q[1], L.q[2], L.q[3], second);
+    bool deg_y = false;
+    const Cons gt = riemann<RK>(plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), 1, g, inv_gm1, deg_y);
+    // x-slope of this lane's cell, then the x-face on its left
+    const Prim ql{shup(qc.rho), shup(qc.u), shup(qc.v), shup(qc.p)};
+    const Prim qr{shdn(qc.rho), shdn(qc.u), shdn(qc.v), shdn(qc.p)};
+    const Prim sx = slope3<LIM>(ql, qc, qr, second);
+    const Prim sxl{shup(sx.rho), shup(sx.u), shup(sx.v), shup(sx.p)};
+    // every lane evaluates the face on its left (lanes 0, 1 and 31 cost
+    // nothing extra in lockstep); only lanes 2..30 use or count theirs
+    bool deg_x = false;
+    const Cons fl = riemann<RK>(plus_half(ql, sxl), minus_half(qc, sx), 0, g, inv_gm1, deg_x);
+    const Cons fr{shdn(fl.rho), shdn(fl.mx), shdn(fl.my), shdn(fl.E)};
+    if (count_deg) {
+      // each face counts once per adjacent cell of this strip in the domain
+      // (count_hllc_degenerate_star_states, explicit_update.hpp:2-56)
+      const bool left_ok = lane >= 3 && lane <= 2 + kCells && x - 1 < nx;
+      if (deg_x && xface) acc.degenerate += (left_ok ? 1 : 0) + (cell_ok ? 1 : 0);
+      if (deg_y && cell_ok) acc.degenerate += 1 + (j + 1 < jend ? 1 : 0);
+    }
+    // update (explicit_update.hpp:92-95) and the reductions of the new state;
+    // all lanes compute, lanes outside the strip or the domain neither store
+    // nor reduce
+    const long long o = static_cast<long long>(j) * P.g.pitch + xs;
+    const long long pl = P.g.plane;
+    Cons n;
+    n.rho = __ldg(u + o) - dt * ((fr.rho - fl.rho) * idx + (gt.rho - gb.rho) * idy);
+    n.mx = __ldg(u + o + pl) - dt * ((fr.mx - fl.mx) * idx + (gt.mx - gb.mx) * idy);
+    n.my = __ldg(u + o + 2 * pl) - dt * ((fr.my - fl.my) * idx + (gt.my - gb.my) * idy);
+    n.E = __ldg(u + o + 3 * pl) - dt * ((fr.E - fl.E) * idx + (gt.E - gb.E) * idy);
+    const Prim q = fast::to_prim_f(n, g);
+    const double cs = fast::fsound_w(q.rho, q.p, g);
+    if (cell_ok) {
+      out[o] = n.rho;
+      out[o + pl] = n.mx;
+      out[o + 2 * pl] = n.my;
+      out[o + 3 * pl] = n.E;
+      const double rate = (fabs(q.u) + cs) * idx + (fabs(q.v) + cs) * idy;
+      if (!isnan(rate)) acc.kmax = umax64(acc.kmax, okey(rate));
+      const bool bad = !isfinite(q.rho) || !isfinite(q.u) || !isfinite(q.v) || !isfinite(q.p) || !isfinite(n.E);
+      acc.krho = umin64(acc.krho, okey(bad ? -kInf : q.rho));
+      acc.kp = umin64(acc.kp, okey(bad ? -kInf : q.p));
+      acc.nonfinite += bad ? 1 : 0;
+    }
+    gb = gt;
+    sy_cur = sy_next;
+  }
+}
+
+template <int RK, int LIM, int H, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __restrict__ out,
                 EcgStepStats* __restrict__ stats, const EcgDtCtl ctl)
 {
   __shared__ BlockRed<WPB * 32> red;
-  const int lane = threadIdx.x & 31;
   const int strip = blockIdx.x * WPB + (threadIdx.x >> 5);
   const int c0 = strip * kCells;
-  const int x = c0 - 2 + lane;
   const int j0 = blockIdx.y * H;
-  const int nx = P.g.nx, ny = P.g.ny;
-  const double g = P.gamma, inv_gm1 = fast::frcp(g - 1.0);
-  const double idx = P.g.inv_dx, idy = P.g.inv_dy;
-  const int lim = P.limiter;
-  const bool second = P.order > 1;
 
   double dt;
   if (!step_control(stats, ctl, dt)) return;
 
-  const bool inner = lane >= 2 && lane < 2 + kCells;   // owns a cell of the strip
-  const bool cell_ok = inner && x < nx;                 // that cell is in the domain
-  const bool xface = lane >= 2 && lane <= 2 + kCells;   // evaluates the x-face on its left
-  unsigned long long kmax = okey(kLowest), krho = okey(kMax), kp = okey(kMax);
-  int nonfinite = 0, degenerate = 0;
-  const int jend = j0 + H < ny ? j0 + H : ny;
-
-  if (c0 < nx) {
-    // ---- prologue: rows j0-2 .. j0+1, y-slopes of rows j0-1 and j0, the y-face below row j0 ----
-    Prim q_m2 = fast::to_prim_f(load_cell(P, u, x, j0 - 2), g);
-    Lane L;
-    L.q[1] = fast::to_prim_f(load_cell(P, u, x, j0 - 1), g);
-    L.q[2] = fast::to_prim_f(load_cell(P, u, x, j0), g);
-    L.q[3] = fast::to_prim_f(load_cell(P, u, x, j0 + 1), g);
-    const Prim sy_m1 = slope3(q_m2, L.q[1], L.q[2], lim, second);
-    Prim sy_cur = slope3(L.q[1], L.q[2], L.q[3], lim, second);
-    Cons gb;
-    {
-      bool deg;
-      gb = riemann<RK>(plus_half(L.q[1], sy_m1), minus_half(L.q[2], sy_cur), 1, g, inv_gm1, deg);
-      if (ctl.count_degenerate && deg && cell_ok && j0 < ny) degenerate += 1;
-    }
-    for (int j = j0; j < jend; ++j) {
-      // window rows j-1 .. j+2
-      L.q[0] = L.q[1];
-      L.q[1] = L.q[2];
-      L.q[2] = L.q[3];
-      L.q[3] = fast::to_prim_f(load_cell(P, u, x, j + 2), g);
-      const Prim& qc = L.q[1];
-      // y-face above row j
-      const Prim sy_next = slope3(L.q[1], L.q[2], L.q[3], lim, second);
-      bool deg_y = false;
-      const Cons gt = riemann<RK>(plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), 1, g, inv_gm1, deg_y);
-      // x-slope of this lane's cell, then the x-face on its left
-      const Prim ql{shup(qc.rho), shup(qc.u), shup(qc.v), shup(qc.p)};
-      const Prim qr{shdn(qc.rho), shdn(qc.u), shdn(qc.v), shdn(qc.p)};
-      const Prim sx = slope3(ql, qc, qr, lim, second);
-      const Prim sxl{shup(sx.rho), shup(sx.u), shup(sx.v), shup(sx.p)};
-      bool deg_x = false;
-      Cons fl{0.0, 0.0, 0.0, 0.0};
-      if (xface) fl = riemann<RK>(plus_half(ql, sxl), minus_half(qc, sx), 0, g, inv_gm1, deg_x);
-      const Cons fr{shdn(fl.rho), shdn(fl.mx), shdn(fl.my), shdn(fl.E)};
-      if (ctl.count_degenerate) {
-        // each face counts once per adjacent cell of this strip in the domain
-        // (count_hllc_degenerate_star_states, explicit_update.hpp:2-56)
-        const bool left_ok = lane >= 3 && lane <= 2 + kCells && x - 1 < nx;
-        if (deg_x && xface) degenerate += (left_ok ? 1 : 0) + (cell_ok ? 1 : 0);
-        if (deg_y && cell_ok) degenerate += 1 + (j + 1 < jend ? 1 : 0);
-      }
-      if (cell_ok) {
-        const long long o = static_cast<long long>(j) * P.g.pitch + x;
-        const long long pl = P.g.plane;
-        Cons n;
-        n.rho = __ldg(u + o) - dt * ((fr.rho - fl.rho) * idx + (gt.rho - gb.rho) * idy);
-        n.mx = __ldg(u + o + pl) - dt * ((fr.mx - fl.mx) * idx + (gt.mx - gb.mx) * idy);
-        n.my = __ldg(u + o + 2 * pl) - dt * ((fr.my - fl.my) * idx + (gt.my - gb.my) * idy);
-        n.E = __ldg(u + o + 3 * pl) - dt * ((fr.E - fl.E) * idx + (gt.E - gb.E) * idy);
-        out[o] = n.rho;
-        out[o + pl] = n.mx;
-        out[o + 2 * pl] = n.my;
-        out[o + 3 * pl] = n.E;
-        const Prim q = fast::to_prim_f(n, g);
-        const double cs = fast::fsound(q.rho, q.p, g);
-        const double rate = (fabs(q.u) + cs) * idx + (fabs(q.v) + cs) * idy;
-        if (!isnan(rate)) kmax = umax64(kmax, okey(rate));
-        const bool bad = !isfinite(q.rho) || !isfinite(q.u) || !isfinite(q.v) || !isfinite(q.p) || !isfinite(n.E);
-        krho = umin64(krho, okey(bad ? -kInf : q.rho));
-        kp = umin64(kp, okey(bad ? -kInf : q.p));
-        nonfinite += bad ? 1 : 0;
-      }
-      gb = gt;
-      sy_cur = sy_next;
-    }
-  }
-  block_commit<WPB * 32>(red, kmax, krho, kp, nonfinite, degenerate, &stats[ctl.acc_slot]);
+  MarchAcc acc;
+  acc.init();
+  if (c0 < P.g.nx) march_strip<RK, LIM, H>(P, u, out, c0, j0, dt, ctl.count_degenerate != 0, acc);
+  block_commit<WPB * 32>(red, acc.kmax, acc.krho, acc.kp, acc.nonfinite, acc.degenerate, &stats[ctl.acc_slot]);
 }
 
-template <int RK, int H>
+template <int RK, int LIM, int H>
 cudaError_t launch_h(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
                      cudaStream_t s)
 {
   constexpr int WPB = 4;
   const int strips = (p.g.nx + kCells - 1) / kCells;
   const dim3 grid((strips + WPB - 1) / WPB, (p.g.ny + H - 1) / H);
-  fv_march_kernel<RK, H, WPB><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl);
+  fv_march_kernel<RK, LIM, H, WPB><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl);
   return cudaGetLastError();
+}
+
+template <int RK, int LIM>
+cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
+                       cudaStream_t s)
+{
+  return p.march_rows == 16 ? launch_h<RK, LIM, 16>(p, in, out, stats, ctl, s)
+                            : launch_h<RK, LIM, 32>(p, in, out, stats, ctl, s);
 }
 
 template <int RK>
 cudaError_t launch_rk(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
                       cudaStream_t s)
 {
-  switch (p.march_rows) {
-    case 8: return launch_h<RK, 8>(p, in, out, stats, ctl, s);
-    case 16: return launch_h<RK, 16>(p, in, out, stats, ctl, s);
-    case 64: return launch_h<RK, 64>(p, in, out, stats, ctl, s);
-    default: return launch_h<RK, 32>(p, in, out, stats, ctl, s);
+  switch (p.limiter) {
+    case ECG_LIMITER_MC: return launch_lim<RK, ECG_LIMITER_MC>(p, in, out, stats, ctl, s);
+    case ECG_LIMITER_VANLEER: return launch_lim<RK, ECG_LIMITER_VANLEER>(p, in, out, stats, ctl, s);
+    default: return launch_lim<RK, ECG_LIMITER_MINMOD>(p, in, out, stats, ctl, s);
   }
 }
 

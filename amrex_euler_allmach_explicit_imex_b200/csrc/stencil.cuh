@@ -93,9 +93,10 @@ __device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsig
 __device__ __forceinline__ unsigned long long umin64(unsigned long long a, unsigned long long b) { return a < b ? a : b; }
 
 // Reduces (max key, min key, min key, count, count) over the block and
-// commits one atomic per quantity into `dst`.
+// commits one atomic per quantity into `dst`.  Thread 0 gets the block's
+// second count back.
 template <int NT>
-__device__ __forceinline__ void block_commit(BlockRed<NT>& red, unsigned long long kmax, unsigned long long kmin1,
+__device__ __forceinline__ int block_commit(BlockRed<NT>& red, unsigned long long kmax, unsigned long long kmin1,
                                              unsigned long long kmin2, int c1, int c2, EcgStepStats* dst)
 {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -129,6 +130,7 @@ __device__ __forceinline__ void block_commit(BlockRed<NT>& red, unsigned long lo
     if (c1) atomicAdd(&dst->nonfinite, c1);
     if (c2) atomicAdd(&dst->degenerate, c2);
   }
+  return c2;
 }
 
 // ---- dt control --------------------------------------------------------------
@@ -451,6 +453,7 @@ cudaError_t launch_fv_rk(const EcgFvParams& p, const double* in, double* out, Ec
 #ifdef ECG_FAST_KERNEL
 #include "fv_fast.cuh"
 #include "fv_march.cuh"
+#include "fv_batch.cuh"
 #endif
 
 cudaError_t launch_fv_step(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
@@ -775,6 +778,91 @@ __device__ Cons exact_ghost(const EcgFvParams& P, const EcgProblem& pr, const do
   return to_cons(q, pr.gamma);
 }
 
+// ---- initial states (initialize_state, problems/problem_initialization.hpp:420-435) ----
+
+// periodic_nearest_delta, problems/problem_state_functions.hpp:32-43
+__device__ double nearest_delta(double x, double c, double lo, double hi)
+{
+  const double L = hi - lo;
+  double d = x - c;
+  if (L > 0.0) d -= L * floor(d / L + 0.5);
+  return d;
+}
+
+// isentropic_vortex_state at t = 0, problem_state_functions.hpp:45-72
+__device__ Prim isentropic_vortex_state(double x, double y, const EcgProblem& c, double plo_x, double plo_y)
+{
+  const double pi = 3.141592653589793238462643383279502884;
+  const double g = c.gamma, s = c.isentropic_vortex_strength;
+  const double dx = nearest_delta(x, c.vortex_cx, plo_x, c.prob_hi_x);
+  const double dy = nearest_delta(y, c.vortex_cy, plo_y, c.prob_hi_y);
+  const double r2 = dx * dx + dy * dy;
+  const double eh = exp(0.5 * (1.0 - r2));
+  const double ef = exp(1.0 - r2);
+  const double temp = 1.0 - (g - 1.0) * s * s / (8.0 * g * pi * pi) * ef;
+  const double rho = c.density_outer * pow(temp, 1.0 / (g - 1.0));
+  const double p = c.pressure * pow(temp, g / (g - 1.0));
+  const double vf = s / (2.0 * pi) * eh;
+  return Prim{rho, c.velocity_x - vf * dy, c.velocity_y + vf * dx, p};
+}
+
+// shock_density_bubble_fraction / _cell_state, problem_initialization.hpp:51-102:
+// post-shock state left of x = 0.2, else ambient p = 1 with the density mixed
+// by the 4 x 4 sub-cell fraction inside the r = 0.2 bubble at (0.5, 0).
+__device__ Prim bubble_cell_state(double x, double y, double dx, double dy)
+{
+  if (x < 0.2) return Prim{2.8181818181818183, 1.6064386578049976, 0.0, 5.0};
+  double inside = 0.0;
+  for (int sy = 0; sy < 4; ++sy) {
+    for (int sx = 0; sx < 4; ++sx) {
+      const double xs = x + ((static_cast<double>(sx) + 0.5) / 4.0 - 0.5) * dx;
+      const double ys = y + ((static_cast<double>(sy) + 0.5) / 4.0 - 0.5) * dy;
+      const double rx = xs - 0.5, ry = ys - 0.0;
+      if (xs >= 0.2 && rx * rx + ry * ry <= 0.2 * 0.2) inside += 1.0;
+    }
+  }
+  const double f = inside / 16.0;
+  return Prim{f * 0.1 + (1.0 - f) * 1.0, 0.0, 0.0, 1.0};
+}
+
+// One thread per cell: the dispatch of initialize_state over the problems.
+__global__ void init_state_kernel(const EcgFvParams P, const EcgProblem pr, double* __restrict__ u)
+{
+  const long long n = static_cast<long long>(P.g.nx) * P.g.ny;
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(e % P.g.nx), j = static_cast<int>(e / P.g.nx);
+    const double x = P.g.plo_x + (static_cast<double>(i) + 0.5) * P.g.dx;
+    const double y = P.g.plo_y + (static_cast<double>(j) + 0.5) * P.g.dy;
+    Cons c;
+    if (pr.problem == ECG_PROBLEM_TORO1) {
+      // initialize_toro (problem_initialization.hpp:265-289): the two states of the test
+      const double* q = x < pr.interface_x ? pr.toro_l : pr.toro_r;
+      c = to_cons(Prim{q[0], q[1], q[2], q[3]}, pr.gamma);
+    } else if (pr.problem == ECG_PROBLEM_GRESHO_VORTEX) {
+      c = to_cons(gresho_state(x, y, pr), pr.gamma);
+    } else if (pr.problem == ECG_PROBLEM_ISENTROPIC_VORTEX) {
+      c = to_cons(isentropic_vortex_state(x, y, pr, P.g.plo_x, P.g.plo_y), pr.gamma);
+    } else if (pr.problem == ECG_PROBLEM_RIEMANN_QUADRANT) {
+      c = to_cons(quadrant_state(x, y, pr), pr.gamma);
+    } else if (pr.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D ||
+               pr.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_CYLINDRICAL) {
+      c = to_cons(bubble_cell_state(x, y, P.g.dx, P.g.dy), pr.gamma);
+    } else {
+      // initialize_blob (problem_initialization.hpp:127-155): top hat, stored directly
+      const double r2 = (x - pr.blob_cx) * (x - pr.blob_cx) + (y - pr.blob_cy) * (y - pr.blob_cy);
+      const double rho = r2 <= pr.blob_radius * pr.blob_radius ? pr.density_inner : pr.density_outer;
+      const double vu = pr.velocity_x, vv = pr.velocity_y;
+      c = Cons{rho, rho * vu, rho * vv, pr.pressure / (pr.gamma - 1.0) + 0.5 * rho * (vu * vu + vv * vv)};
+    }
+    const long long o = static_cast<long long>(j) * P.g.pitch + i;
+    u[o] = c.rho;
+    u[o + P.g.plane] = c.mx;
+    u[o + 2 * P.g.plane] = c.my;
+    u[o + 3 * P.g.plane] = c.E;
+  }
+}
+
 // Writes the ghosted box [-2, nx+2) x [-2, ny+2) as fill_problem_ghosts
 // leaves it.  only_ring: write the out-of-domain cells only (the ghost ring
 // read by the stencil kernels under exact-state Dirichlet policies).
@@ -821,6 +909,13 @@ cudaError_t launch_ghost_box(const EcgFvParams& p, const EcgProblem& pr, const d
 {
   const long long n = static_cast<long long>(p.g.nx + 4) * (p.g.ny + 4);
   ghost_box_kernel<<<reduce_blocks(n, 256), 256, 0, s>>>(p, pr, u, time, stats, k, out, opitch, oplane, only_ring);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_state(const EcgFvParams& p, const EcgProblem& pr, double* u, cudaStream_t s)
+{
+  const long long n = static_cast<long long>(p.g.nx) * p.g.ny;
+  init_state_kernel<<<reduce_blocks(n, 256), 256, 0, s>>>(p, pr, u);
   return cudaGetLastError();
 }
 

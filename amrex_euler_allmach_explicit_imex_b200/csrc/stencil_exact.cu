@@ -6,4 +6,5 @@
 
 const EcgStencilOps ecg_exact_ops = {ecg_exact::launch_fv_step,   ecg_exact::launch_state_reduce,
                                      ecg_exact::launch_ghost_box, ecg_exact::launch_init_stats,
-                                     ecg_exact::launch_init_state_stats, ecg_exact::launch_seed_stats};
+                                     ecg_exact::launch_init_state_stats, ecg_exact::launch_seed_stats,
+                                     ecg_exact::launch_init_state};

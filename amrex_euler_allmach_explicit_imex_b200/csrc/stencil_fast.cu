@@ -6,4 +6,5 @@
 
 const EcgStencilOps ecg_fast_ops = {ecg_fast::launch_fv_step,   ecg_fast::launch_state_reduce,
                                     ecg_fast::launch_ghost_box, ecg_fast::launch_init_stats,
-                                    ecg_fast::launch_init_state_stats, ecg_fast::launch_seed_stats};
+                                    ecg_fast::launch_init_state_stats, ecg_fast::launch_seed_stats,
+                                    ecg_fast::launch_init_state};

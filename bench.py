@@ -271,13 +271,10 @@ def run_ours(args):
 
     cfg = read_config(WORKLOAD_KV).cfg
     stream = torch.cuda.Stream(device=dev)
-    from tests.oracle import Oracle
-
-    # initial state from the reference problem initializer (restated in the
-    # oracle; the product does not depend on it)
-    u0 = Oracle().initialize(cfg)
     ctx = api.Context(cfg, arith="fast", device=local, stream=stream.cuda_stream)
-    ctx.upload(u0)
+    # the problem's initial condition, written on the device (initialize_state)
+    api.initialize_state(ctx)
+    u0 = ctx.download()  # host copy for the end-to-end leg
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     cells = NX * NY
 

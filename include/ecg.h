@@ -304,6 +304,12 @@ ecg_status ecg_upload_state_device(ecg_ctx* ctx, const double* base, int32_t lo_
                                    int64_t jstride, int64_t nstride);
 ecg_status ecg_download_state_device(ecg_ctx* ctx, double* base, int32_t lo_x, int32_t lo_y,
                                      int64_t jstride, int64_t nstride);
+/* initialize_state (problems/problem_initialization.hpp:420-435): writes the
+ * problem's initial condition into the context's state on the device (one
+ * kernel; no host data).  Transcendental profiles (Gresho, isentropic vortex)
+ * agree with the reference to rounding of log/exp/pow; the others exactly in
+ * ECG_ARITH_EXACT. */
+ecg_status ecg_initialize_state(ecg_ctx* ctx);
 /* Fills the whole ghosted box [-2, nx+2) x [-2, ny+2) (4 planes, jstride
  * nx+4, nstride (nx+4)(ny+4)) as fill_problem_ghosts does
  * (problems/boundary_conditions.hpp:202-219). */

@@ -163,3 +163,31 @@ def test_full_size_bubble_matches_oracle_on_a_band(gpu, oracle):
         u1 = ctx.download()
     assert np.array_equal(u1, ref_u1)
     assert deg == ref_deg
+
+
+INIT_PROBLEMS = [
+    ("toro1", "geometry.prob_hi=1 0.1\namr.n_cell=37 5\nprob.test=3\n", 0.0),
+    ("gresho_vortex", "amr.n_cell=33 29\neuler.mach=0.01\n", 1e-14),
+    ("isentropic_vortex", "amr.n_cell=40 24\ngeometry.prob_lo=-5 -5\ngeometry.prob_hi=5 5\n"
+                          "euler.vortex_center=0 0\n", 1e-14),
+    ("riemann_quadrant", "amr.n_cell=30 30\n", 0.0),
+    ("shock_density_bubble_2d", "amr.n_cell=160 40\ngeometry.prob_hi=2 0.5\n", 0.0),
+    ("advection_blob", "amr.n_cell=45 45\n", 0.0),
+]
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+@pytest.mark.parametrize("problem,extra,tol", INIT_PROBLEMS, ids=[p for p, _, _ in INIT_PROBLEMS])
+def test_initialize_state_on_device(gpu, oracle, arith, problem, extra, tol):
+    """initialize_state on the device against the oracle's restatement of
+    problem_initialization.hpp: exact where the profile needs only + - * /
+    sqrt (in ECG_ARITH_EXACT), to rounding of log/exp/pow otherwise."""
+    cfg = read_config(f"euler.problem={problem}\n" + extra).cfg
+    want = oracle.initialize(cfg)
+    with api.Context(cfg, arith=arith) as ctx:
+        api.initialize_state(ctx)
+        got = ctx.download()
+    if arith == "exact" and tol == 0.0:
+        assert np.array_equal(got, want)
+    else:
+        assert golden_io.state_rel_err(got, want) <= max(tol, 1e-15)

@@ -110,3 +110,22 @@ def test_live_reference_random_states(oracle, ref):
         a, na = ref.step(st, dt)
         b, nb = oracle.step(cfg, st, dt)
         assert np.array_equal(a, b) and na == nb
+
+
+INIT_KV = [
+    "euler.problem=toro1\ngeometry.prob_hi=1 0.1\namr.n_cell=37 5\nprob.test=3\n",
+    "euler.problem=gresho_vortex\namr.n_cell=33 29\neuler.mach=0.01\n",
+    "euler.problem=isentropic_vortex\namr.n_cell=40 24\ngeometry.prob_lo=-5 -5\ngeometry.prob_hi=5 5\n"
+    "euler.vortex_center=0 0\n",
+    "euler.problem=riemann_quadrant\namr.n_cell=30 30\n",
+    "euler.problem=shock_density_bubble_2d\namr.n_cell=160 40\ngeometry.prob_hi=2 0.5\n",
+    "euler.problem=advection_blob\namr.n_cell=45 45\n",
+]
+
+
+@pytest.mark.parametrize("kv", INIT_KV, ids=lambda s: s.split("\n")[0].split("=")[1])
+def test_oracle_initialize_matches_reference(oracle, ref, kv):
+    """The restated initialize_state is bit-identical to the reference's
+    (problems/problem_initialization.hpp:420-435) for every problem."""
+    cfg = ref.configure(kv)
+    assert np.array_equal(oracle.initialize(cfg), ref.initialize())
