@@ -30,7 +30,14 @@ from ._lib import EcgError, check, load
 from .config import RunSettings, read_config
 
 
+# cudaStreamLegacy: the legacy default stream, which torch's default stream is
+_LEGACY_STREAM = 1
+
+
 def gpu_options(arith="fast", imex_precision="fp64", device=0, tile_y=0, stream=None, **kw):
+    """ecg_gpu_options.  stream: None for a context-owned stream, or a
+    cudaStream_t handle; 0 (torch's default stream) selects the legacy default
+    stream, so the context's work is ordered with torch's default-stream work."""
     lib = load()
     o = abi.GpuOptions()
     lib.ecg_default_gpu_options(C.byref(o))
@@ -38,7 +45,7 @@ def gpu_options(arith="fast", imex_precision="fp64", device=0, tile_y=0, stream=
     o.arith = abi.ARITH_EXACT if arith == "exact" else abi.ARITH_FAST
     o.imex_precision = abi.IMEX_MIXED if imex_precision == "mixed" else abi.IMEX_FP64
     o.tile_y = tile_y
-    o.stream = stream
+    o.stream = _LEGACY_STREAM if stream == 0 else stream
     for k, v in kw.items():
         setattr(o, k, v)
     return o

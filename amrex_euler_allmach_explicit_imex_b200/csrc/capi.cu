@@ -147,6 +147,7 @@ EcgFvParams fv_params(ecg_ctx* c, bool imex_policy)
   p.limiter = c->cfg.slope_limiter;
   p.riemann = c->cfg.riemann;
   p.march_rows = c->opt.tile_x;
+  p.sm_count = c->num_sms;
   return p;
 }
 

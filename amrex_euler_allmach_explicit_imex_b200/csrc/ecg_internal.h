@@ -53,7 +53,9 @@ struct EcgFvParams {
   long long ring_pitch, ring_plane;
   double gamma;
   int order, limiter, riemann;
-  int march_rows;            // rows per warp of the column-strip kernel (8, 16, 32, 64; 0: default)
+  int march_rows;            // rows per warp of the column-strip kernel (0: sized to fill one wave)
+  int sm_count;              // SMs of the device (0: 148)
+  int pad;
 };
 
 // Per-step reduction record.  Keys are order-preserving integer images of

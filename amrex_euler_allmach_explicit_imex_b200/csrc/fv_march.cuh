@@ -68,10 +68,10 @@ struct MarchAcc {
 // Advances the strip of 28 cells starting at column c0 over rows
 // [j0, min(j0 + H, ny)) from u into out.  Called by all 32 lanes of a warp
 // (the flux helpers vote across the warp).
-template <int RK, int LIM, int H>
+template <int RK, int LIM>
 __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* __restrict__ u,
-                                            double* __restrict__ out, int c0, int j0, double dt, bool count_deg,
-                                            MarchAcc& acc)
+                                            double* __restrict__ out, int c0, int j0, int H, double dt,
+                                            bool count_deg, MarchAcc& acc)
 {
   const int lane = threadIdx.x & 31;
   const int x = c0 - 2 + lane;
@@ -156,10 +156,10 @@ __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* 
   }
 }
 
-template <int RK, int LIM, int H, int WPB>
+template <int RK, int LIM, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
 fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __restrict__ out,
-                EcgStepStats* __restrict__ stats, const EcgDtCtl ctl)
+                EcgStepStats* __restrict__ stats, const EcgDtCtl ctl, const int H)
 {
   __shared__ BlockRed<WPB * 32> red;
   const int strip = blockIdx.x * WPB + (threadIdx.x >> 5);
@@ -171,27 +171,37 @@ fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __res
 
   MarchAcc acc;
   acc.init();
-  if (c0 < P.g.nx) march_strip<RK, LIM, H>(P, u, out, c0, j0, dt, ctl.count_degenerate != 0, acc);
+  if (c0 < P.g.nx) march_strip<RK, LIM>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc);
   block_commit<WPB * 32>(red, acc.kmax, acc.krho, acc.kp, acc.nonfinite, acc.degenerate, &stats[ctl.acc_slot]);
 }
 
-template <int RK, int LIM, int H>
-cudaError_t launch_h(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
-                     cudaStream_t s)
-{
-  constexpr int WPB = 4;
-  const int strips = (p.g.nx + kCells - 1) / kCells;
-  const dim3 grid((strips + WPB - 1) / WPB, (p.g.ny + H - 1) / H);
-  fv_march_kernel<RK, LIM, H, WPB><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl);
-  return cudaGetLastError();
-}
-
+// Rows per warp: the given march_rows, else the smallest count that lets all
+// warp strips of the grid run in a single wave of resident warps (so no SM
+// idles in a tail), at least 8 so the per-strip prologue stays cheap.
 template <int RK, int LIM>
 cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
                        cudaStream_t s)
 {
-  return p.march_rows == 16 ? launch_h<RK, LIM, 16>(p, in, out, stats, ctl, s)
-                            : launch_h<RK, LIM, 32>(p, in, out, stats, ctl, s);
+  constexpr int WPB = 4;
+  const int strips = (p.g.nx + kCells - 1) / kCells;
+  int H = p.march_rows;
+  if (H <= 0) {
+    static int blocks_per_sm = 0;
+    if (blocks_per_sm == 0) {
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fv_march_kernel<RK, LIM, WPB>, WPB * 32, 0) != cudaSuccess ||
+          b < 1)
+        b = 1;
+      blocks_per_sm = b;
+    }
+    const long long slots = static_cast<long long>(p.sm_count > 0 ? p.sm_count : 148) * blocks_per_sm * WPB;
+    const long long per_col = slots / strips;  // warps available per strip column
+    H = per_col > 0 ? static_cast<int>((p.g.ny + per_col - 1) / per_col) : p.g.ny;
+    if (H < 8) H = 8;
+  }
+  const dim3 grid((strips + WPB - 1) / WPB, (p.g.ny + H - 1) / H);
+  fv_march_kernel<RK, LIM, WPB><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl, H);
+  return cudaGetLastError();
 }
 
 template <int RK>

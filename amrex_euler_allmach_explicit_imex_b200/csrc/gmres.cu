@@ -35,8 +35,10 @@
 
 namespace {
 
-constexpr int NT = 256;
-constexpr int kResidualBlocks = 148 * 8;  // grid of residual_kernel
+// 512 threads per block (one block per SM): 16 warps in flight for the
+// latency-bound dot products and basis updates, within 128 registers a thread.
+constexpr int NT = 512;
+constexpr int kResidualBlocks = 148 * 2;  // grid of residual_kernel
 constexpr double kEps = 2.220446049250313e-16;
 
 struct GridBar {
@@ -169,8 +171,8 @@ __device__ __forceinline__ Rows own_rows(long long n)
 
 // Shared-memory layout of one block (doubles): six vectors of m+8 (Givens
 // cosines/sines, rotated rhs g, current Hessenberg column, reduced values,
-// update coefficients), per-warp partials (m+8) x NW, and NT + m + 8 scratch
-// (grid reductions stage at most max(NT, m + 8) values).
+// update coefficients), per-warp partials of one sum (NW), and NT + m + 8
+// scratch (grid reductions stage at most max(NT, m + 8) values).
 constexpr int NW = NT / 32;
 struct Smem {
   double* cs;
@@ -193,27 +195,27 @@ __device__ __forceinline__ Smem carve(double* base, int m)
   s.red = s.hcol + L;
   s.coef = s.red + L;
   s.wpart = s.coef + L;
-  s.scratch = s.wpart + L * NW;
+  s.scratch = s.wpart + NW;
   return s;
 }
-inline size_t smem_bytes(int m) { return sizeof(double) * (static_cast<size_t>(7 + NW) * (m + 8) + NT); }
+inline size_t smem_bytes(int m) { return sizeof(double) * (static_cast<size_t>(7) * (m + 8) + NW + NT); }
 
-// Per-thread value v of sum q -> per-warp partial (lane 0 stores).
-__device__ __forceinline__ void warp_partial(double v, int q, double* wpart)
+// Per-thread value v of one sum -> per-warp partial (lane 0 stores).
+__device__ __forceinline__ void warp_partial(double v, double* wpart)
 {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) wpart[q * NW + (threadIdx.x >> 5)] = v;
+  if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = v;
 }
 
-// part_row[q] = sum of the warp partials of q in warp order, q < cnt.
-__device__ __forceinline__ void commit_partials(const double* wpart, int cnt, double* part_row)
+// *dst = sum of the warp partials in warp order.
+__device__ __forceinline__ void commit_partial(const double* wpart, double* dst)
 {
   __syncthreads();
-  for (int q = threadIdx.x; q < cnt; q += NT) {
+  if (threadIdx.x == 0) {
     double s = 0.0;
-    for (int w = 0; w < NW; ++w) s += wpart[q * NW + w];
-    part_row[q] = s;
+    for (int w = 0; w < NW; ++w) s += wpart[w];
+    *dst = s;
   }
   __syncthreads();
 }
@@ -321,9 +323,20 @@ __device__ __forceinline__ void block_dots(const T* __restrict__ V, long long n,
   for (int i = warp; i < tot; i += NW) {
     double s = 0.0;
     if (i < nvec) {
+      // 8 rows a lane per pass, all loads issued before the first use
       const T* vi = V + static_cast<long long>(i) * n;
-#pragma unroll 4
-      for (long long q = rw.r0 + lane; q < rw.r1; q += 32) s += static_cast<double>(vi[q]) * static_cast<double>(__ldcg(w + q));
+      for (long long base = rw.r0 + lane; base < rw.r1; base += 32 * 8) {
+        T a[8], b[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const long long q = base + 32LL * k;
+          const bool ok = q < rw.r1;
+          a[k] = ok ? __ldcg(vi + q) : T(0);
+          b[k] = ok ? w[q] : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += static_cast<double>(a[k]) * static_cast<double>(b[k]);
+      }
     } else if (i == nvec) {
 #pragma unroll 4
       for (long long q = rw.r0 + lane; q < rw.r1; q += 32) {
@@ -382,8 +395,8 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
     }
     block_max_partial(bmax, part_row, 0, S.scratch);
     block_max_partial(rmax, part_row, 1, S.scratch);
-    warp_partial(r2, 0, S.wpart);
-    commit_partials(S.wpart, 1, part_row + 2);
+    warp_partial(r2, S.wpart);
+    commit_partial(S.wpart, part_row + 2);
   }
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
     st.timeout = 1;
@@ -478,6 +491,7 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
       for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
         double wv = static_cast<double>(w[q]);
+#pragma unroll 8
         for (int i = 0; i <= j; ++i) wv -= S.coef[i] * static_cast<double>(V[static_cast<long long>(i) * n + q]);
         w[q] = static_cast<T>(wv);
       }
@@ -536,6 +550,7 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
     double rmx = 0.0;
     for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
       double wv = static_cast<double>(w[q]);
+#pragma unroll 8
       for (int i = 0; i <= j; ++i) wv -= S.coef[i] * static_cast<double>(V[static_cast<long long>(i) * n + q]);
       const T vq = static_cast<T>(wv * inv_nn);
       vn[q] = vq;
@@ -578,8 +593,10 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
   if (ynf) st.nonfinite = 1;
   for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
     double xv = static_cast<double>(x0vec[q]);
-    if (!ynf)
+    if (!ynf) {
+#pragma unroll 8
       for (int i = 0; i < k; ++i) xv += y[i] * static_cast<double>(V[static_cast<long long>(i) * n + q]);
+    }
     xvec[q] = static_cast<T>(xv);
   }
   return st;

@@ -13,7 +13,9 @@ admissibility diagnostics.
 
 value: cell-updates/s with the state resident in HBM (CUDA events around each
 step on the launching stream; L2 flushed before every timed step by writing a
-256 MiB buffer, since the 52 MB state would otherwise stay in the 126 MB L2).
+256 MiB buffer and reading it back, since the 52 MB state would otherwise stay
+in the 126 MB L2; the read-back leaves clean lines, so the step does not pay
+for writing back the flush buffer).
 e2e: the same metric through the C ABI with HOST buffers: each step uploads the
 caller's state from pinned host memory (ecg_upload_state), steps, and
 downloads it (ecg_download_state), as a drop-in for a host-resident MultiFab
@@ -24,6 +26,13 @@ headers built with g++ against a single-box AMReX shim) on
 the same workload, on this machine's host cores (rows split over all host
 threads); one step = the driver's loop
 body compute_euler_dt -> euler_fv_one_step -> compute_diagnostics.
+
+Two more measurements ride on the same JSON line at N=1 (skip them with
+--no-extra-legs): "imex", the second half of the metric (Gresho 256^2,
+M = 0.01, IMEX T1/S2: ms per step of the all-FP64 GMRES solve and of the
+FP32-inner / FP64-refined solve, and the relative drift between the two
+states), and "batched" (64 seeded Riemann solves of uneven sizes advanced by
+one persistent launch per step for 200 steps).
 
 Multi-GPU: the single 2560x640 solve does not shard without a halo exchange,
 so N GPUs run N independent replicas (weak scaling); value is the sum over
@@ -64,7 +73,7 @@ CONFIG = {
     "grid": [NX, NY],
     "domain": [[0.0, 2.0], [0.0, 0.5]],
     "riemann": "hllc",
-    "l2": "flushed before every timed step (256 MiB write)",
+    "l2": "flushed before every timed step (256 MiB written, then read back)",
     "parallelism": "replicas",
 }
 
@@ -80,7 +89,7 @@ def peaks():
 
 def profile_traffic():
     """DRAM bytes per launch of the step kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "fv_step_hllc_bubble_2560x640.json")
+    p = os.path.join(ROOT, "profiles", "fv_march_hllc_bubble_2560x640.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f).get("dram_bytes_per_launch")
@@ -257,6 +266,79 @@ def run_reference_arm(args):
 # GPU arm
 
 
+IMEX_KV = {
+    "amr.n_cell": "256 256", "geometry.is_periodic": "1 1", "euler.problem": "gresho_vortex",
+    "euler.vortex_center": "0.5 0.5", "euler.mach": 0.01, "euler.pressure": 1.0 / (1.4 * 0.01 * 0.01),
+    "euler.method": "imex", "euler.spatial_order": 2, "euler.imex_acoustic_startup": 0,
+    "euler.imex_picard_iterations": 4, "euler.imex_solver_tol": "1e-10", "euler.imex_solver_max_iter": 200,
+    "euler.imex_cfl": 0.4, "stop_time": 1.0,
+}
+
+
+def imex_leg(dev, stream, steps=3):
+    """Gresho 256^2, M = 0.01, IMEX T1/S2 (4 Picard solves, GMRES tol 1e-10):
+    time per step of the all-FP64 solve and of the FP32-inner / FP64-refined
+    solve on the same GPU, and the relative drift between their states."""
+    import torch
+
+    from amrex_euler_allmach_explicit_imex_b200 import api
+    from amrex_euler_allmach_explicit_imex_b200.config import read_config
+
+    cfg = read_config(IMEX_KV).cfg
+    out = {}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        with api.Context(cfg, imex_precision=prec, device=dev.index or 0, stream=stream.cuda_stream) as ctx:
+            api.initialize_state(ctx)
+            t = 0.0
+            ms, its = [], []
+            for k in range(steps + 1):
+                dt, _ = api.compute_imex_dt(ctx, t)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                d = api.euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, dt)
+                b.record(stream)
+                b.synchronize()
+                if k > 0:
+                    ms.append(a.elapsed_time(b))
+                    its.append(d.solver_iterations)
+                t += dt
+            states[prec] = ctx.download()
+            out[prec] = {"ms_per_step": statistics.median(ms), "gmres_iterations": its,
+                         "status": api.solver_status_str(d.solver_status)}
+    drift = float(np.abs(states["fp64"] - states["mixed"]).max() / np.abs(states["fp64"]).max())
+    return {"workload": "gresho_vortex 256x256 periodic, M=0.01, IMEX T1/S2, 4 Picard, GMRES tol 1e-10",
+            "steps_timed": steps, "fp64": out["fp64"], "mixed": out["mixed"],
+            "mixed_speedup": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"], "state_rel_drift": drift}
+
+
+def batch_leg(dev, steps=200):
+    """64 independent explicit O2 HLLC Riemann solves on the seeded grid ladder
+    {64x64, 128x32, 256x256, 512x128, 1024x256}, one persistent launch per
+    step for the whole batch, CUDA graphs; cell-updates/s over `steps` steps."""
+    import torch
+
+    from amrex_euler_allmach_explicit_imex_b200 import api, workloads
+
+    cfgs, states = workloads.riemann_batch(64, seed=0)
+    cells = sum(c.cfg.n_cell[0] * c.cfg.n_cell[1] for c in cfgs)
+    with api.Batch(cfgs, device=dev.index or 0) as b:
+        for k, u in enumerate(states):
+            b.upload(k, u)
+        b.run(24)  # autotune and graph capture
+        for k, u in enumerate(states):
+            b.upload(k, u)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = b.run(steps)
+        el = time.perf_counter() - t0
+    ok = all(r.steps == steps and r.failed == 0 for r in res)
+    return {"workload": "64 Riemann solves, grids drawn (seed 0) from 64x64..1024x256, O2 HLLC FP64, CFL 0.5",
+            "cells": cells, "steps": steps, "seconds": el, "value": cells * steps / el, "unit": UNIT,
+            "all_solves_completed": ok}
+
+
 def run_ours(args):
     import torch
 
@@ -276,6 +358,7 @@ def run_ours(args):
     api.initialize_state(ctx)
     u0 = ctx.download()  # host copy for the end-to-end leg
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    flush_sink = torch.empty((), dtype=torch.float32, device=dev)
     cells = NX * NY
 
     def one_step(t):
@@ -295,9 +378,14 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         torch.cuda.synchronize(dev)
         for k in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(float(k))
             dt = api.compute_euler_dt(ctx, t)  # host read of the previous step's fused CFL reduction
+            with torch.cuda.stream(stream):
+                # write then read 256 MiB: no line of the state stays in L2,
+                # and no dirty line is left for the step to write back; the
+                # step is queued behind the flush, so the events time the
+                # kernel, not the host's launch of it
+                flush.fill_(float(k))
+                flush_sink.copy_(flush.sum())
             ev[k][0].record(stream)
             api.euler_fv_one_step(ctx, dt, t)
             ev[k][1].record(stream)
@@ -350,7 +438,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (the reference's own shock-density-bubble initializer)", "config": CONFIG,
+            "data": "synthetic (the shock-density-bubble initial condition of the reference's initialize_state, written on the device)", "config": CONFIG,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_source": peak_kind,
                          "note": "algorithmic bytes = 64 B x 1,638,400 cells per launch; event time of the fused step kernel"},
@@ -361,6 +449,9 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "state_ok": bool(ok),
         }
+        if world == 1 and not args.no_extra_legs:
+            line["imex"] = imex_leg(dev, stream)
+            line["batched"] = batch_leg(dev)
         print(json.dumps(line))
     ctx.close()
     if dist is not None:
@@ -377,11 +468,23 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-legs", action="store_true", help="skip the IMEX and batched measurements")
+    ap.add_argument("--only", choices=["imex", "batched"], default=None,
+                    help="run one of the extra legs alone (profiling) and print its JSON")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.only:
+        import torch
+
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        stream = torch.cuda.Stream(device=dev)
+        leg = imex_leg(dev, stream, steps=2) if args.only == "imex" else batch_leg(dev)
+        print(json.dumps({"leg": args.only, **leg}))
+        return 0
     return run_ours(args)
 
 

@@ -138,7 +138,7 @@ typedef struct ecg_gpu_options {
   int32_t mixed_inner_max_iter;  /* FP32 inner iterations per refinement sweep */
   double mixed_inner_rtol;       /* FP32 inner relative residual target */
   int32_t mixed_max_refinements; /* outer FP64 refinement sweeps */
-  int32_t tile_x;           /* column-strip kernel: rows each warp marches (8, 16, 32, 64; 0 default) */
+  int32_t tile_x;           /* column-strip kernel: rows each warp marches (0: sized so the grid fills one wave) */
   int32_t tile_y;           /* explicit kernel: 0 default, 1 square 16x16 tiles,
                                8 or 16 the 32 x tile_y tile kernel */
   void* stream;             /* cudaStream_t to run on, NULL = context-owned stream */
