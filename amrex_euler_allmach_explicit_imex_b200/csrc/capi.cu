@@ -364,9 +364,10 @@ ecg_status ecg_create(ecg_ctx** out, const ecg_run_config* cfg, const ecg_gpu_op
   c->grid.inv_dy = 1.0 / c->grid.dy;
   c->grid.plo_x = cfg->prob_lo[0];
   c->grid.plo_y = cfg->prob_lo[1];
-  // kernel choice: 0 default (fast build: column-strip marching kernel; exact
-  // build: 32x16 tile), 1 square 16x16 tile (fast build), 8 or 16: 32xTY tile
-  c->tile_y = (o.tile_y == 1 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
+  // kernel choice: 0 default (fast build: column-strip kernel with paired
+  // faces; exact build: 32x16 tile), 2 column strips with faces one at a time,
+  // 1 square 16x16 tile (fast build), 8 or 16: 32xTY tile
+  c->tile_y = (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
   const size_t sbytes = sizeof(double) * 4 * c->grid.plane;
   bool ok = true;
   if (o.stream) {

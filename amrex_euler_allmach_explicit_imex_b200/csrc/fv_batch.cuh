@@ -91,7 +91,8 @@ fv_batch_kernel(const EcgBatchSolve* __restrict__ solves, EcgStepStats* __restri
     march::MarchAcc acc;
     acc.init();
     if (c0 < S.p.g.nx)
-      march::march_strip<RK, LIM>(S.p, S.u[par], S.u[par ^ 1], c0, j0, H, s_dt, ctl.count_degenerate != 0, acc);
+      march::march_strip<RK, LIM, true>(S.p, S.u[par], S.u[par ^ 1], c0, j0, H, s_dt, ctl.count_degenerate != 0,
+                                        acc);
     const int deg = block_commit<WPB * 32>(red, acc.kmax, acc.krho, acc.kp, acc.nonfinite, acc.degenerate,
                                            &stats[3 * s + ctl.acc_slot]);
     if (threadIdx.x == 0 && deg != 0) atomicAdd(&degenerate_total[s], static_cast<unsigned long long>(deg));

@@ -197,6 +197,72 @@ __device__ __forceinline__ Cons hllc_w(const Prim& l, const Prim& r, int axis, d
   return out;
 }
 
+// Sound speed on the rsqrt path only; `bad` marks states outside (0, 1e300)
+// whose speed must come from the IEEE formula instead.
+__device__ __forceinline__ double fsound_core(double rho, double p, double g, bool& bad)
+{
+  const double t = g * p;
+  const double q = t * rho;
+  bad = !pos_normal_range(q);
+  return t * frsqrt(q);
+}
+
+// hllc_w without any warp vote: the branch-free HLLC flux of states whose
+// sound speeds are on the rsqrt path and whose star state is not degenerate.
+// `fallback` marks the faces that must be recomputed by hllc_f instead
+// (degenerate star state or a sound speed off the rsqrt path), so two faces
+// can be evaluated back to back and repaired by one vote.
+__device__ __forceinline__ Cons hllc_core(const Prim& l, const Prim& r, int axis, double g, double inv_gm1,
+                                          bool& fallback)
+{
+  const double unl = normal_vel(l, axis), unr = normal_vel(r, axis);
+  bool bl, br;
+  const double cl = fsound_core(l.rho, l.p, g, bl), cr = fsound_core(r.rho, r.p, g, br);
+  const double sl = smin(unl - cl, unr - cr), sr = smax(unl + cl, unr + cr);
+  const bool ordered = sl < sr;
+  const bool sup_l = sl >= 0.0, sup_r = sr <= 0.0;
+  const bool supersonic = ordered && (sup_l || sup_r);
+  const double al = l.rho * (sl - unl), ar = r.rho * (sr - unr);
+  const double den = al - ar;
+  const double sm = fdiv(r.p - l.p + al * unl - ar * unr, den);
+  const double lsd = sl - sm, rsd = sr - sm;
+  const bool deg = !ordered || (!supersonic && (fabs(den) <= 1.0e-12 || fabs(lsd) <= 1.0e-12 || fabs(rsd) <= 1.0e-12));
+  fallback = deg || bl || br;
+  const bool left = supersonic ? sup_l : sm >= 0.0;
+  const Prim q = left ? l : r;
+  const double s = left ? sl : sr, un = left ? unl : unr, a = left ? al : ar;
+  const Cons u = to_cons_f(q, inv_gm1);
+  const Cons f = pflux(q, u, axis);
+  const double ps = 0.5 * (l.p + al * (sm - unl) + r.p + ar * (sm - unr));
+  const double inv_sd = frcp(left ? lsd : rsd);
+  const double rs = a * inv_sd;
+  const double es = ((s - un) * u.E - q.p * un + ps * sm) * inv_sd;
+  const double tang = axis == 0 ? q.v : q.u;
+  const double smx = axis == 0 ? rs * sm : rs * tang;
+  const double smy = axis == 0 ? rs * tang : rs * sm;
+  Cons out;
+  out.rho = supersonic ? f.rho : fma(s, rs - u.rho, f.rho);
+  out.mx = supersonic ? f.mx : fma(s, smx - u.mx, f.mx);
+  out.my = supersonic ? f.my : fma(s, smy - u.my, f.my);
+  out.E = supersonic ? f.E : fma(s, es - u.E, f.E);
+  return out;
+}
+
+// rusanov_i on the rsqrt path; `fallback` as for hllc_core.
+__device__ __forceinline__ Cons rusanov_core(const Prim& l, const Prim& r, int axis, double g, double inv_gm1,
+                                             bool& fallback)
+{
+  const Cons ul = to_cons_f(l, inv_gm1), ur = to_cons_f(r, inv_gm1);
+  const Cons fl = pflux(l, ul, axis), fr = pflux(r, ur, axis);
+  bool bl, br;
+  const double cl = fsound_core(l.rho, l.p, g, bl), cr = fsound_core(r.rho, r.p, g, br);
+  fallback = bl || br;
+  const double sm = smax(fabs(normal_vel(l, axis)) + cl, fabs(normal_vel(r, axis)) + cr);
+  const double hs = 0.5 * sm;
+  return Cons{0.5 * (fl.rho + fr.rho) - hs * (ur.rho - ul.rho), 0.5 * (fl.mx + fr.mx) - hs * (ur.mx - ul.mx),
+              0.5 * (fl.my + fr.my) - hs * (ur.my - ul.my), 0.5 * (fl.E + fr.E) - hs * (ur.E - ul.E)};
+}
+
 // low_mach_correct_velocity_states (reconstruction_fluxes.hpp:212-232), fast arithmetic.
 __device__ __forceinline__ void lowmach_f(Prim& l, Prim& r, double g)
 {

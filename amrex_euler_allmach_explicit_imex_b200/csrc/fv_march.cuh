@@ -43,13 +43,57 @@ __device__ __forceinline__ Prim minus_half(const Prim& q, const Prim& s)
   return Prim{fma(-0.5, s.rho, q.rho), fma(-0.5, s.u, q.u), fma(-0.5, s.v, q.v), fma(-0.5, s.p, q.p)};
 }
 
+// The x-face and the y-face of a row, evaluated back to back on the fast
+// path (independent instruction streams the scheduler can interleave); faces
+// that need the reference path (degenerate HLLC star state, sound speed off
+// the rsqrt path) are recomputed after one warp vote.  deg_*: HLLC fell back
+// to Rusanov on that face.
 template <int RK>
-__device__ __forceinline__ Cons riemann(Prim L, Prim R, int axis, double g, double inv_gm1, bool& deg)
+__device__ __forceinline__ void face_pair(Prim xl, Prim xr, Prim yl, Prim yr, double g, double inv_gm1, Cons& fx,
+                                          Cons& fy, bool& deg_x, bool& deg_y)
+{
+  if (RK == ECG_RIEMANN_LOWMACH_HLLC) {
+    fast::lowmach_f(xl, xr, g);
+    fast::lowmach_f(yl, yr, g);
+  }
+  bool bx, by;
+  if (RK == ECG_RIEMANN_RUSANOV) {
+    fx = fast::rusanov_core(xl, xr, 0, g, inv_gm1, bx);
+    fy = fast::rusanov_core(yl, yr, 1, g, inv_gm1, by);
+  } else {
+    fx = fast::hllc_core(xl, xr, 0, g, inv_gm1, bx);
+    fy = fast::hllc_core(yl, yr, 1, g, inv_gm1, by);
+  }
+  deg_x = deg_y = false;
+  if (__any_sync(0xffffffffu, bx || by)) {
+    if (RK == ECG_RIEMANN_RUSANOV) {
+      if (bx) fx = fast::rusanov_f(xl, xr, 0, g, inv_gm1);
+      if (by) fy = fast::rusanov_f(yl, yr, 1, g, inv_gm1);
+    } else {
+      if (bx) fx = fast::hllc_f(xl, xr, 0, g, inv_gm1, deg_x);
+      if (by) fy = fast::hllc_f(yl, yr, 1, g, inv_gm1, deg_y);
+    }
+  }
+}
+
+// One face with the warp-voting flux (faces evaluated one after the other).
+template <int RK>
+__device__ __forceinline__ Cons face_w(Prim l, Prim r, int axis, double g, double inv_gm1, bool& deg)
 {
   deg = false;
-  if (RK == ECG_RIEMANN_RUSANOV) return fast::rusanov_i(L, R, axis, g, inv_gm1);
-  if (RK == ECG_RIEMANN_LOWMACH_HLLC) fast::lowmach_f(L, R, g);
-  return fast::hllc_w(L, R, axis, g, inv_gm1, deg);
+  if (RK == ECG_RIEMANN_RUSANOV) return fast::rusanov_i(l, r, axis, g, inv_gm1);
+  if (RK == ECG_RIEMANN_LOWMACH_HLLC) fast::lowmach_f(l, r, g);
+  return fast::hllc_w(l, r, axis, g, inv_gm1, deg);
+}
+
+// One face on its own (the y-face below the first row of a strip).
+template <int RK>
+__device__ __forceinline__ Cons face_one(Prim l, Prim r, int axis, double g, double inv_gm1, bool& deg)
+{
+  deg = false;
+  if (RK == ECG_RIEMANN_RUSANOV) return fast::rusanov_f(l, r, axis, g, inv_gm1);
+  if (RK == ECG_RIEMANN_LOWMACH_HLLC) fast::lowmach_f(l, r, g);
+  return fast::hllc_f(l, r, axis, g, inv_gm1, deg);
 }
 
 // Reductions of one warp strip over the new state.
@@ -68,7 +112,7 @@ struct MarchAcc {
 // Advances the strip of 28 cells starting at column c0 over rows
 // [j0, min(j0 + H, ny)) from u into out.  Called by all 32 lanes of a warp
 // (the flux helpers vote across the warp).
-template <int RK, int LIM>
+template <int RK, int LIM, bool PAIR>
 __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* __restrict__ u,
                                             double* __restrict__ out, int c0, int j0, int H, double dt,
                                             bool count_deg, MarchAcc& acc)
@@ -96,7 +140,7 @@ __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* 
   Cons gb;
   {
     bool deg;
-    gb = riemann<RK>(plus_half(L.q[1], sy_m1), minus_half(L.q[2], sy_cur), 1, g, inv_gm1, deg);
+    gb = face_one<RK>(plus_half(L.q[1], sy_m1), minus_half(L.q[2], sy_cur), 1, g, inv_gm1, deg);
     if (count_deg && deg && cell_ok && j0 < ny) acc.degenerate += 1;
   }
   for (int j = j0; j < jend; ++j) {
@@ -106,19 +150,24 @@ __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* 
     L.q[2] = L.q[3];
     L.q[3] = fast::to_prim_f(load_cell(P, u, x, j + 2), g);
     const Prim& qc = L.q[1];
-    // y-face above row j
+    // slopes: y of row j+1 (for the y-face above row j), x of this lane's cell
     const Prim sy_next = slope3<LIM>(L.q[1], L.q[2], L.q[3], second);
-    bool deg_y = false;
-    const Cons gt = riemann<RK>(plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), 1, g, inv_gm1, deg_y);
-    // x-slope of this lane's cell, then the x-face on its left
     const Prim ql{shup(qc.rho), shup(qc.u), shup(qc.v), shup(qc.p)};
     const Prim qr{shdn(qc.rho), shdn(qc.u), shdn(qc.v), shdn(qc.p)};
     const Prim sx = slope3<LIM>(ql, qc, qr, second);
     const Prim sxl{shup(sx.rho), shup(sx.u), shup(sx.v), shup(sx.p)};
-    // every lane evaluates the face on its left (lanes 0, 1 and 31 cost
-    // nothing extra in lockstep); only lanes 2..30 use or count theirs
-    bool deg_x = false;
-    const Cons fl = riemann<RK>(plus_half(ql, sxl), minus_half(qc, sx), 0, g, inv_gm1, deg_x);
+    // the x-face on this lane's left and the y-face above row j; every lane
+    // evaluates both (lanes 0, 1 and 31 cost nothing extra in lockstep), only
+    // lanes 2..30 use or count their x-face
+    Cons fl, gt;
+    bool deg_x, deg_y;
+    if (PAIR) {
+      face_pair<RK>(plus_half(ql, sxl), minus_half(qc, sx), plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), g,
+                    inv_gm1, fl, gt, deg_x, deg_y);
+    } else {
+      gt = face_w<RK>(plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), 1, g, inv_gm1, deg_y);
+      fl = face_w<RK>(plus_half(ql, sxl), minus_half(qc, sx), 0, g, inv_gm1, deg_x);
+    }
     const Cons fr{shdn(fl.rho), shdn(fl.mx), shdn(fl.my), shdn(fl.E)};
     if (count_deg) {
       // each face counts once per adjacent cell of this strip in the domain
@@ -156,7 +205,7 @@ __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* 
   }
 }
 
-template <int RK, int LIM, int WPB>
+template <int RK, int LIM, int WPB, bool PAIR>
 __global__ void __launch_bounds__(WPB * 32)
 fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __restrict__ out,
                 EcgStepStats* __restrict__ stats, const EcgDtCtl ctl, const int H)
@@ -171,14 +220,14 @@ fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __res
 
   MarchAcc acc;
   acc.init();
-  if (c0 < P.g.nx) march_strip<RK, LIM>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc);
+  if (c0 < P.g.nx) march_strip<RK, LIM, PAIR>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc);
   block_commit<WPB * 32>(red, acc.kmax, acc.krho, acc.kp, acc.nonfinite, acc.degenerate, &stats[ctl.acc_slot]);
 }
 
 // Rows per warp: the given march_rows, else the smallest count that lets all
 // warp strips of the grid run in a single wave of resident warps (so no SM
 // idles in a tail), at least 8 so the per-strip prologue stays cheap.
-template <int RK, int LIM>
+template <int RK, int LIM, bool PAIR>
 cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
                        cudaStream_t s)
 {
@@ -189,7 +238,7 @@ cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgS
     static int blocks_per_sm = 0;
     if (blocks_per_sm == 0) {
       int b = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fv_march_kernel<RK, LIM, WPB>, WPB * 32, 0) != cudaSuccess ||
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fv_march_kernel<RK, LIM, WPB, PAIR>, WPB * 32, 0) != cudaSuccess ||
           b < 1)
         b = 1;
       blocks_per_sm = b;
@@ -200,29 +249,37 @@ cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgS
     if (H < 8) H = 8;
   }
   const dim3 grid((strips + WPB - 1) / WPB, (p.g.ny + H - 1) / H);
-  fv_march_kernel<RK, LIM, WPB><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl, H);
+  fv_march_kernel<RK, LIM, WPB, PAIR><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl, H);
   return cudaGetLastError();
 }
 
-template <int RK>
+template <int RK, bool PAIR>
 cudaError_t launch_rk(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
                       cudaStream_t s)
 {
   switch (p.limiter) {
-    case ECG_LIMITER_MC: return launch_lim<RK, ECG_LIMITER_MC>(p, in, out, stats, ctl, s);
-    case ECG_LIMITER_VANLEER: return launch_lim<RK, ECG_LIMITER_VANLEER>(p, in, out, stats, ctl, s);
-    default: return launch_lim<RK, ECG_LIMITER_MINMOD>(p, in, out, stats, ctl, s);
+    case ECG_LIMITER_MC: return launch_lim<RK, ECG_LIMITER_MC, PAIR>(p, in, out, stats, ctl, s);
+    case ECG_LIMITER_VANLEER: return launch_lim<RK, ECG_LIMITER_VANLEER, PAIR>(p, in, out, stats, ctl, s);
+    default: return launch_lim<RK, ECG_LIMITER_MINMOD, PAIR>(p, in, out, stats, ctl, s);
   }
 }
 
+// pair: evaluate the x- and y-face of a row together (one vote for both);
+// otherwise one after the other.
 inline cudaError_t launch(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
-                          const EcgDtCtl& ctl, cudaStream_t s)
+                          const EcgDtCtl& ctl, cudaStream_t s, bool pair)
 {
   switch (p.riemann) {
-    case ECG_RIEMANN_RUSANOV: return launch_rk<ECG_RIEMANN_RUSANOV>(p, in, out, stats, ctl, s);
-    case ECG_RIEMANN_LOWMACH_HLLC: return launch_rk<ECG_RIEMANN_LOWMACH_HLLC>(p, in, out, stats, ctl, s);
+    case ECG_RIEMANN_RUSANOV:
+      return pair ? launch_rk<ECG_RIEMANN_RUSANOV, true>(p, in, out, stats, ctl, s)
+                  : launch_rk<ECG_RIEMANN_RUSANOV, false>(p, in, out, stats, ctl, s);
+    case ECG_RIEMANN_LOWMACH_HLLC:
+      return pair ? launch_rk<ECG_RIEMANN_LOWMACH_HLLC, true>(p, in, out, stats, ctl, s)
+                  : launch_rk<ECG_RIEMANN_LOWMACH_HLLC, false>(p, in, out, stats, ctl, s);
     case ECG_RIEMANN_XIE_AM_HLLC_P: return fast::launch(p, in, out, stats, ctl, s);  // needs the 5-face sensor
-    default: return launch_rk<ECG_RIEMANN_HLLC>(p, in, out, stats, ctl, s);
+    default:
+      return pair ? launch_rk<ECG_RIEMANN_HLLC, true>(p, in, out, stats, ctl, s)
+                  : launch_rk<ECG_RIEMANN_HLLC, false>(p, in, out, stats, ctl, s);
   }
 }
 

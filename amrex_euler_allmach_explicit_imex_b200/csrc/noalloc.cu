@@ -166,7 +166,7 @@ ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gp
   if (st != ECG_OK) return st;
 
   const EcgStencilOps* ops = o.arith == ECG_ARITH_EXACT ? &ecg_exact_ops : &ecg_fast_ops;
-  const int tile_y = (o.tile_y == 1 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
+  const int tile_y = (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
   cudaStream_t s = static_cast<cudaStream_t>(o.stream);
 
   // grid of ecg_create with the caller's strides

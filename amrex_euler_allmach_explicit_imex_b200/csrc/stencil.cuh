@@ -460,8 +460,10 @@ cudaError_t launch_fv_step(const EcgFvParams& p, const double* in, double* out, 
                            const EcgDtCtl& ctl, int tile_y, cudaStream_t s)
 {
 #ifdef ECG_FAST_KERNEL
-  // 0: column-strip marching kernel (default); 1: square-tile kernel
-  if (tile_y == 0) return march::launch(p, in, out, stats, ctl, s);
+  // 0: column-strip kernel, x- and y-faces evaluated together (default);
+  // 2: column-strip kernel, faces one after the other; 1: square-tile kernel
+  if (tile_y == 0) return march::launch(p, in, out, stats, ctl, s, true);
+  if (tile_y == 2) return march::launch(p, in, out, stats, ctl, s, false);
   if (tile_y == 1) return fast::launch(p, in, out, stats, ctl, s);
 #endif
   switch (p.riemann) {

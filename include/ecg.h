@@ -139,8 +139,9 @@ typedef struct ecg_gpu_options {
   double mixed_inner_rtol;       /* FP32 inner relative residual target */
   int32_t mixed_max_refinements; /* outer FP64 refinement sweeps */
   int32_t tile_x;           /* column-strip kernel: rows each warp marches (0: sized so the grid fills one wave) */
-  int32_t tile_y;           /* explicit kernel: 0 default, 1 square 16x16 tiles,
-                               8 or 16 the 32 x tile_y tile kernel */
+  int32_t tile_y;           /* explicit kernel: 0 default (column strips, x- and y-faces
+                               evaluated together), 2 column strips with faces one at a
+                               time, 1 square 16x16 tiles, 8 or 16 the 32 x tile_y tiles */
   void* stream;             /* cudaStream_t to run on, NULL = context-owned stream */
 } ecg_gpu_options;
 
