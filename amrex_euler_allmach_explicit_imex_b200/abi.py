@@ -202,6 +202,7 @@ PROBLEM = {
     "isentropic_vortex": 4,
     "shock_density_bubble_2d": 5,
     "shock_density_bubble_cylindrical_clawpack": 6,
+    "shock_bubble_mach122": 7,  # no counterpart in the reference (ecg.h)
 }
 RIEMANN = {"rusanov": 0, "hllc": 1, "lowmach_hllc": 2, "xie_am_hllc_p": 3}
 METHOD = {"explicit": 0, "imex": 1}

@@ -102,6 +102,9 @@ def parse_problem(v):
     if s in ("shock_density_bubble_cylindrical_clawpack", "shock_density_bubble_cylindrical",
              "clawpack_shock_density_bubble"):
         return abi.PROBLEM["shock_density_bubble_cylindrical_clawpack"]
+    if s in ("shock_bubble_mach122", "shock_density_bubble_mach122"):
+        # the [0,4]x[0,1] Mach 1.22 configuration; no ProblemKind in the reference
+        return abi.PROBLEM["shock_bubble_mach122"]
     raise ConfigError("Unknown euler.problem=" + v)
 
 
@@ -373,4 +376,23 @@ def read_config(source=None):
         else:
             if c.problem == abi.PROBLEM["shock_density_bubble_cylindrical_clawpack"]:
                 raise ConfigError("cylindrical shock_density_bubble IMEX is not part of the cleaned Cartesian code pack.")
+    if c.problem == abi.PROBLEM["shock_bubble_mach122"]:
+        # defaults and checks of the Mach 1.22 shock / bubble configuration
+        if (c.prob_lo[0] == 0.0 and c.prob_lo[1] == 0.0 and c.prob_hi[0] == 1.0 and c.prob_hi[1] == 1.0):
+            c.prob_hi[0], c.prob_hi[1] = 4.0, 1.0
+        if c.stop_time == 0.05:
+            c.stop_time = 1.0
+        if c.cfl == 0.4:
+            c.cfl = 0.45
+        if c.spatial_order == 1:
+            c.spatial_order = 2
+        c.is_periodic[0], c.is_periodic[1] = 0, 0
+        ok = (abs(c.prob_lo[0]) < 1e-14 and abs(c.prob_hi[0] - 4.0) < 1e-14 and abs(c.prob_lo[1]) < 1e-14
+              and abs(c.prob_hi[1] - 1.0) < 1e-14)
+        if not ok:
+            raise ConfigError("shock_bubble_mach122 requires domain x=[0,4], y=[0,1].")
+        if abs(c.gamma - 1.4) > 1e-14:
+            raise ConfigError("shock_bubble_mach122 is a same-gamma ideal-gas test with gamma=1.4.")
+        if c.method != abi.METHOD["explicit"]:
+            raise ConfigError("shock_bubble_mach122 runs the explicit method only.")
     return s

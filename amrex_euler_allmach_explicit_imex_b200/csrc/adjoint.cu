@@ -64,7 +64,14 @@ __device__ Src source_of(const EcgFvParams& P, int i, int j)
     }
   } else if (j >= ny) {
     if (P.bc.y_hi == BC_CONST) return Src{0, 0, false, false};
-    s.j = P.bc.y_hi == BC_PERIODIC ? wrapi(j, ny) : ny - 1;
+    if (P.bc.y_hi == BC_PERIODIC) {
+      s.j = wrapi(j, ny);
+    } else if (P.bc.y_hi == BC_REFLECT) {
+      s.j = 2 * ny - 1 - j < 0 ? 0 : 2 * ny - 1 - j;
+      s.flip = true;
+    } else {
+      s.j = ny - 1;
+    }
   }
   return s;
 }

@@ -119,6 +119,20 @@ void make_bc(const ecg_run_config& c, bool outflow_only, EcgBc& bc, EcgProblem& 
     bc.y_hi = BC_CLAMP;
     return;
   }
+  if (c.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122) {
+    // post-shock inflow on the left, outflow on the right, walls at y = 0 and y = 1
+    mach122_post_shock(c.gamma, pr.post_shock);
+    const double* q = pr.post_shock;
+    bc.x_lo = BC_CONST;
+    bc.cst[0] = q[0];
+    bc.cst[1] = q[0] * q[1];
+    bc.cst[2] = q[0] * q[2];
+    bc.cst[3] = q[3] / (c.gamma - 1.0) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2]);
+    bc.x_hi = BC_CLAMP;
+    bc.y_lo = BC_REFLECT;
+    bc.y_hi = BC_REFLECT;
+    return;
+  }
   if (outflow_only) return;
   const bool exact = c.field_boundary == ECG_FIELD_BOUNDARY_EXACT_DIRICHLET && (!pr.periodic_x || !pr.periodic_y);
   if (!exact) return;

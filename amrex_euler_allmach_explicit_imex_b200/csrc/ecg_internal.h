@@ -44,7 +44,27 @@ struct EcgProblem {
   double blob_cx, blob_cy, blob_radius, velocity_x, velocity_y;
   double isentropic_vortex_strength;
   double prob_hi_x, prob_hi_y;
+  double post_shock[4];  // primitive post-shock state of ECG_PROBLEM_SHOCK_BUBBLE_MACH122
 };
+
+// Mach 1.22 shock / bubble configuration (ECG_PROBLEM_SHOCK_BUBBLE_MACH122).
+constexpr double kM122Mach = 1.22;
+constexpr double kM122ShockX = 0.5;
+constexpr double kM122BubbleX = 1.0, kM122BubbleY = 0.5, kM122BubbleR = 0.25, kM122BubbleRho = 0.138;
+
+// Rankine-Hugoniot state behind a shock of Mach number m running into
+// (rho, u, p) = (1, 0, 1) at rest: {rho, u, v, p}.
+inline void mach122_post_shock(double gamma, double q[4])
+{
+  const double m2 = kM122Mach * kM122Mach;
+  const double rho2 = (gamma + 1.0) * m2 / ((gamma - 1.0) * m2 + 2.0);
+  const double p2 = 1.0 + 2.0 * gamma * (m2 - 1.0) / (gamma + 1.0);
+  const double s = kM122Mach * __builtin_sqrt(gamma);
+  q[0] = rho2;
+  q[1] = s * (1.0 - 1.0 / rho2);
+  q[2] = 0.0;
+  q[3] = p2;
+}
 
 struct EcgFvParams {
   EcgGrid g;

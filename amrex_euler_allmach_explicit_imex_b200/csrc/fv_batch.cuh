@@ -57,7 +57,7 @@ __device__ __forceinline__ bool solve_control(EcgStepStats* __restrict__ st, con
 }
 
 template <int RK, int LIM, int H, int WPB>
-__global__ void __launch_bounds__(WPB * 32)
+__global__ void __launch_bounds__(WPB * 32, 16 / WPB)
 fv_batch_kernel(const EcgBatchSolve* __restrict__ solves, EcgStepStats* __restrict__ stats,
                 unsigned long long* __restrict__ degenerate_total, const int* __restrict__ max_step,
                 const EcgBatchCtl ctl)

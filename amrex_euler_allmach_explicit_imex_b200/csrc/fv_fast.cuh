@@ -4,10 +4,9 @@
 // Included inside the ecg_fast namespace of stencil.cuh.
 //
 //  * Division and square root: the PTX approximations rcp.approx.ftz.f64 and
-//    rsqrt.approx.ftz.f64 refined by two Newton-Raphson steps, and a final
-//    residual correction for quotients (Markstein, "Computation of elementary
-//    functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 1990).
-//    Results are within a few units in the last place of the IEEE values.
+//    rsqrt.approx.ftz.f64 (about 2^-20 relative, measured on B200) refined by
+//    one third-order Householder step each, which takes the error to a few
+//    units in the last place; a quotient is a * (1/b).
 //  * Sound speed sqrt(g p / rho) = (g p) * rsqrt(g p rho): no division.
 //  * HLLC star state: one reciprocal of (s_K - s_M) for density and energy.
 //  * MUSCL: the limited slope of every cell and axis is computed once per
@@ -16,30 +15,26 @@
 //    x-face and one y-face, so no thread idles at the face barrier.
 namespace fast {
 
+// 1/b: the hardware approximation (about 2^-20 relative) refined by one
+// third-order step y (1 + e + e^2), e = 1 - b y (error about e^3).
 __device__ __forceinline__ double frcp(double b)
 {
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-  double e = fma(-b, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-b, y, 1.0);
-  return fma(y, e, y);
+  const double e = fma(-b, y, 1.0);
+  return fma(y, fma(e, e, e), y);
 }
 
-__device__ __forceinline__ double fdiv(double a, double b)
-{
-  const double y = frcp(b);
-  const double q = a * y;
-  return fma(fma(-b, q, a), y, q);
-}
+__device__ __forceinline__ double fdiv(double a, double b) { return a * frcp(b); }
 
+// 1/sqrt(x): the hardware approximation refined by one third-order step
+// y (1 + e/2 + 3e^2/8), e = 1 - x y^2.
 __device__ __forceinline__ double frsqrt(double x)
 {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  const double h = 0.5 * x;
-  y = y * fma(-h * y, y, 1.5);
-  return y * fma(-h * y, y, 1.5);
+  const double e = fma(-x * y, y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
 }
 
 // sqrt(x) for x > 0 via x * rsqrt(x); IEEE sqrt for 0, negative, inf, NaN.

@@ -72,7 +72,15 @@ __device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __
     }
   } else if (j >= ny) {
     if (P.bc.y_hi == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
-    j = P.bc.y_hi == BC_PERIODIC ? wrapi(j, ny) : ny - 1;
+    if (P.bc.y_hi == BC_PERIODIC) {
+      j = wrapi(j, ny);
+    } else if (P.bc.y_hi == BC_REFLECT) {
+      j = 2 * ny - 1 - j;  // row ny + k mirrors row ny - 1 - k
+      j = j < 0 ? 0 : j;
+      flip = true;
+    } else {
+      j = ny - 1;
+    }
   }
   const long long o = static_cast<long long>(j) * P.g.pitch + i;
   const long long pl = P.g.plane;
@@ -827,6 +835,25 @@ __device__ Prim bubble_cell_state(double x, double y, double dx, double dy)
   return Prim{f * 0.1 + (1.0 - f) * 1.0, 0.0, 0.0, 1.0};
 }
 
+// Mach 1.22 shock / bubble cell: post-shock state left of the shock, else
+// ambient (1, 0, 0, 1) with the bubble density mixed by its 4 x 4 sub-cell
+// area fraction (the sampling of shock_density_bubble_fraction).
+__device__ Prim mach122_cell_state(double x, double y, double dx, double dy, const double* post_shock)
+{
+  if (x < kM122ShockX) return Prim{post_shock[0], post_shock[1], post_shock[2], post_shock[3]};
+  double inside = 0.0;
+  for (int sy = 0; sy < 4; ++sy) {
+    for (int sx = 0; sx < 4; ++sx) {
+      const double xs = x + ((static_cast<double>(sx) + 0.5) / 4.0 - 0.5) * dx;
+      const double ys = y + ((static_cast<double>(sy) + 0.5) / 4.0 - 0.5) * dy;
+      const double rx = xs - kM122BubbleX, ry = ys - kM122BubbleY;
+      if (xs >= kM122ShockX && rx * rx + ry * ry <= kM122BubbleR * kM122BubbleR) inside += 1.0;
+    }
+  }
+  const double f = inside / 16.0;
+  return Prim{f * kM122BubbleRho + (1.0 - f) * 1.0, 0.0, 0.0, 1.0};
+}
+
 // One thread per cell: the dispatch of initialize_state over the problems.
 __global__ void init_state_kernel(const EcgFvParams P, const EcgProblem pr, double* __restrict__ u)
 {
@@ -847,6 +874,8 @@ __global__ void init_state_kernel(const EcgFvParams P, const EcgProblem pr, doub
       c = to_cons(isentropic_vortex_state(x, y, pr, P.g.plo_x, P.g.plo_y), pr.gamma);
     } else if (pr.problem == ECG_PROBLEM_RIEMANN_QUADRANT) {
       c = to_cons(quadrant_state(x, y, pr), pr.gamma);
+    } else if (pr.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122) {
+      c = to_cons(mach122_cell_state(x, y, P.g.dx, P.g.dy, pr.post_shock), pr.gamma);
     } else if (pr.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D ||
                pr.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_CYLINDRICAL) {
       c = to_cons(bubble_cell_state(x, y, P.g.dx, P.g.dy), pr.gamma);

@@ -45,7 +45,14 @@ typedef enum ecg_problem {
   ECG_PROBLEM_RIEMANN_QUADRANT = 3,
   ECG_PROBLEM_ISENTROPIC_VORTEX = 4,
   ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D = 5,
-  ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_CYLINDRICAL = 6
+  ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_CYLINDRICAL = 6,
+  /* No counterpart in ProblemKind: a Mach 1.22 planar shock at x = 0.5 running
+   * into (rho, p) = (1, 1) and a circular bubble (r = 0.25 at (1, 0.5),
+   * rho = 0.138, p = 1) on [0,4] x [0,1], post-shock inflow on the left,
+   * outflow on the right, reflecting walls at y = 0 and y = 1, gamma = 1.4.
+   * The reference's config reader rejects this geometry for
+   * shock_density_bubble_2d (config_reader.hpp:288-298). Explicit method only. */
+  ECG_PROBLEM_SHOCK_BUBBLE_MACH122 = 7
 } ecg_problem;
 
 /* Mirrors RiemannKind (core/solver_types.hpp:11). */

@@ -154,6 +154,36 @@ Prim bubble_cell(double x, double y, double dx, double dy)
   return Prim{f * 0.1 + (1.0 - f) * 1.0, 0.0, 0.0, 1.0};
 }
 
+// Mach 1.22 shock / bubble configuration (ECG_PROBLEM_SHOCK_BUBBLE_MACH122,
+// no ProblemKind in the reference): Rankine-Hugoniot state behind a Mach 1.22
+// shock into (rho, u, p) = (1, 0, 1), gamma = 1.4; the same sub-cell bubble
+// sampling as shock_density_bubble_fraction with the shock at x = 0.5 and a
+// rho = 0.138 bubble of radius 0.25 at (1, 0.5).
+Prim mach122_post_shock(double gamma)
+{
+  const double mach = 1.22;
+  const double m2 = mach * mach;
+  const double rho2 = (gamma + 1.0) * m2 / ((gamma - 1.0) * m2 + 2.0);
+  const double p2 = 1.0 + 2.0 * gamma * (m2 - 1.0) / (gamma + 1.0);
+  const double s = mach * std::sqrt(gamma);
+  return Prim{rho2, s * (1.0 - 1.0 / rho2), 0.0, p2};
+}
+Prim mach122_cell(double x, double y, double dx, double dy, double gamma)
+{
+  if (x < 0.5) return mach122_post_shock(gamma);
+  double inside = 0.0;
+  for (int sy = 0; sy < 4; ++sy) {
+    for (int sx = 0; sx < 4; ++sx) {
+      const double xs = x + ((static_cast<double>(sx) + 0.5) / 4.0 - 0.5) * dx;
+      const double ys = y + ((static_cast<double>(sy) + 0.5) / 4.0 - 0.5) * dy;
+      const double rx = xs - 1.0, ry = ys - 0.5;
+      if (xs >= 0.5 && rx * rx + ry * ry <= 0.25 * 0.25) inside += 1.0;
+    }
+  }
+  const double f = inside / 16.0;
+  return Prim{f * 0.138 + (1.0 - f) * 1.0, 0.0, 0.0, 1.0};
+}
+
 // reference_sound_speed / velocity_scale_from_mach, state_primitives.hpp:207-215
 inline double vel_scale(const ecg_run_config& c)
 {
@@ -353,6 +383,7 @@ void initialize(const ecg_run_config& c, Grid& gr)
         case ECG_PROBLEM_RIEMANN_QUADRANT: q = quadrant(x, y, c); break;
         case ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D:
         case ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_CYLINDRICAL: q = bubble_cell(x, y, geo.dx, geo.dy); break;
+        case ECG_PROBLEM_SHOCK_BUBBLE_MACH122: q = mach122_cell(x, y, geo.dx, geo.dy, c.gamma); break;
         default: {
           const double r2 = (x - c.blob_cx) * (x - c.blob_cx) + (y - c.blob_cy) * (y - c.blob_cy);
           const double rho = r2 <= c.blob_radius * c.blob_radius ? c.density_inner : c.density_outer;
@@ -422,6 +453,28 @@ void fill_bubble(Grid& g, const Geo& geo, double gamma)
     }
 }
 
+// Mach 1.22 configuration: post-shock inflow left, copy right, mirror walls
+// (-rho v) at y = 0 and y = 1.
+void fill_mach122(Grid& g, double gamma)
+{
+  const Cons left = to_cons(mach122_post_shock(gamma), gamma);
+  for (int j = -2; j < g.ny + 2; ++j)
+    for (int i = -2; i < g.nx + 2; ++i) {
+      const bool ox = i < 0 || i >= g.nx, oy = j < 0 || j >= g.ny;
+      if (!ox && !oy) continue;
+      if (i < 0) { g.set(i, j, left); continue; }
+      const int ii = i >= g.nx ? g.nx - 1 : i;
+      int jj = j;
+      bool refl = false;
+      if (j < 0) { jj = -j - 1; refl = true; }
+      else if (j >= g.ny) { jj = 2 * g.ny - 1 - j; refl = true; }
+      jj = clampi(jj, g.ny);
+      Cons c = g.cons(ii, jj);
+      if (refl) c.my = -c.my;
+      g.set(i, j, c);
+    }
+}
+
 // exact-state Dirichlet fills, boundary_conditions.hpp:133-163,
 // problem_initialization.hpp:209-263,308-375
 void fill_exact(Grid& g, const Geo& geo, const ecg_run_config& c, double time)
@@ -469,6 +522,8 @@ void fill_ghosts(Grid& g, const ecg_run_config& c, double time)
   const bool exact = c.field_boundary == ECG_FIELD_BOUNDARY_EXACT_DIRICHLET && (!geo.per[0] || !geo.per[1]);
   if (is_bubble(c)) {
     fill_bubble(g, geo, c.gamma);
+  } else if (c.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122) {
+    fill_mach122(g, c.gamma);
   } else if (exact && (c.problem == ECG_PROBLEM_GRESHO_VORTEX || c.problem == ECG_PROBLEM_TORO1 ||
                        c.problem == ECG_PROBLEM_RIEMANN_QUADRANT || c.problem == ECG_PROBLEM_ADVECTION_BLOB)) {
     fill_exact(g, geo, c, time);

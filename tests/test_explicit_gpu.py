@@ -191,3 +191,29 @@ def test_initialize_state_on_device(gpu, oracle, arith, problem, extra, tol):
         assert np.array_equal(got, want)
     else:
         assert golden_io.state_rel_err(got, want) <= max(tol, 1e-15)
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+@pytest.mark.parametrize("riemann", ["hllc", "xie_am_hllc_p"])
+def test_mach122_variant_steps(gpu, oracle, arith, riemann):
+    """The Mach 1.22 shock / bubble configuration: device initial state and
+    three steps against the oracle's restatement (bit-identical in
+    ECG_ARITH_EXACT, 1e-12 relative per step in ECG_ARITH_FAST)."""
+    cfg = read_config(f"euler.problem=shock_bubble_mach122\namr.n_cell=96 24\neuler.riemann={riemann}\n").cfg
+    u = oracle.initialize(cfg)
+    with api.Context(cfg, arith=arith) as ctx:
+        api.initialize_state(ctx)
+        assert np.array_equal(ctx.download(), u) if arith == "exact" else golden_io.state_rel_err(ctx.download(), u) <= 1e-15
+        ctx.upload(u)
+        t = 0.0
+        for _ in range(3):
+            dt = oracle.euler_dt(cfg, u, t)
+            want, _ = oracle.step(cfg, u, dt, t)
+            ctx.upload(u)
+            api.euler_fv_one_step(ctx, dt, t)
+            got = ctx.download()
+            if arith == "exact":
+                assert np.array_equal(got, want)
+            else:
+                assert golden_io.state_rel_err(got, want) <= FAST_TOL
+            u, t = want, t + dt

@@ -129,3 +129,27 @@ def test_oracle_initialize_matches_reference(oracle, ref, kv):
     (problems/problem_initialization.hpp:420-435) for every problem."""
     cfg = ref.configure(kv)
     assert np.array_equal(oracle.initialize(cfg), ref.initialize())
+
+
+def test_oracle_mach122_configuration(oracle):
+    """The Mach 1.22 shock / bubble configuration (no ProblemKind in the
+    reference): Rankine-Hugoniot post-shock state left of x = 0.5, the
+    rho = 0.138 bubble at (1, 0.5), reflecting walls at y = 0 and y = 1."""
+    cfg = read_config("euler.problem=shock_bubble_mach122\namr.n_cell=64 16\n").cfg
+    u = oracle.initialize(cfg)
+    g, m = 1.4, 1.22
+    rho2 = (g + 1) * m * m / ((g - 1) * m * m + 2)
+    p2 = 1 + 2 * g * (m * m - 1) / (g + 1)
+    u2 = m * np.sqrt(g) * (1 - 1 / rho2)
+    assert u[0, 5, 3] == pytest.approx(rho2, rel=1e-15)          # x = 0.1875 < 0.5
+    assert u[1, 5, 3] == pytest.approx(rho2 * u2, rel=1e-15)
+    assert u[3, 5, 3] == pytest.approx(p2 / (g - 1) + 0.5 * rho2 * u2 * u2, rel=1e-15)
+    assert u[0, 8, 16] == pytest.approx(0.138)                     # (1.03, 0.53): inside the bubble
+    assert u[0, 2, 60] == 1.0 and u[3, 2, 60] == pytest.approx(2.5)  # ambient
+    # walls: ghost row -1 mirrors row 0, ghost row ny mirrors row ny-1, my negated
+    w = np.array(u)
+    w[2] = 0.1 + 0.01 * np.arange(64)[None, :] * np.ones((16, 1))
+    gh = oracle.fill_ghosts(cfg, w)
+    assert np.array_equal(gh[2, 1, 2:-2], -w[2, 0]) and np.array_equal(gh[2, 0, 2:-2], -w[2, 1])
+    assert np.array_equal(gh[2, -2, 2:-2], -w[2, -1]) and np.array_equal(gh[2, -1, 2:-2], -w[2, -2])
+    assert np.array_equal(gh[0, 2:-2, 0], np.full(16, rho2))      # inflow column
