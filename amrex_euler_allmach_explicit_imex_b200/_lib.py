@@ -34,6 +34,7 @@ SIGNATURES = {
     "ecg_fill_problem_ghosts": (C.c_int, [_CTX, _D, _P]),
     "ecg_synchronize": (C.c_int, [_CTX]),
     "ecg_initialize_state": (C.c_int, [_CTX]),
+    "ecg_paper_t1s2_run": (C.c_int, [_CTX, C.POINTER(abi.PaperOptions), C.POINTER(abi.PaperResult)]),
     "ecg_euler_fv_one_step": (C.c_int, [_CTX, _D, _D, C.POINTER(_I32)]),
     "ecg_compute_euler_dt": (C.c_int, [_CTX, _D, C.POINTER(_D)]),
     "ecg_compute_imex_dt": (C.c_int, [_CTX, _D, C.POINTER(_D), C.POINTER(abi.ImexTimestepDiag)]),

@@ -182,6 +182,52 @@ class RunResult(C.Structure):
     ]
 
 
+class PaperOptions(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32),
+        ("max_steps", C.c_int32),
+        ("epsilon", C.c_double),
+        ("fixed_dt", C.c_double),
+    ]
+
+
+class PaperResult(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int32),
+        ("solver_failure_count", C.c_int32),
+        ("gmres_iterations_max", C.c_int32),
+        ("enthalpy_guard_count", C.c_int32),
+        ("nonfinite_count", C.c_int32),
+        ("nonpositive_count", C.c_int32),
+        ("passed", C.c_int32),
+        ("pad", C.c_int32),
+        ("final_time", C.c_double),
+        ("pressure_residual_linf_max", C.c_double),
+        ("pressure_relative_residual_linf_max", C.c_double),
+        ("rho_min", C.c_double),
+        ("pressure_min", C.c_double),
+        ("density_l1_error", C.c_double),
+        ("velocity_l1_error", C.c_double),
+        ("pressure_l1_error", C.c_double),
+        ("density_l2_error", C.c_double),
+        ("velocity_l2_error", C.c_double),
+        ("pressure_l2_error", C.c_double),
+        ("density_linf_error", C.c_double),
+        ("pressure_linf_error", C.c_double),
+    ]
+
+
+# euler.bdltv20_paper_t1_s2 settings (ecg_paper_mode)
+PAPER_MODE = {
+    "off": 0,
+    "toro_x_exact_dirichlet_y_periodic_2d": 1,
+    "toro_xy_exact_dirichlet_2d": 2,
+    "gresho_exact_dirichlet_2d": 3,
+    "isentropic_vortex_periodic_2d": 4,
+    "advection_blob_periodic_2d": 5,
+}
+
+
 class BatchResult(C.Structure):
     _fields_ = [
         ("steps", C.c_int32),

@@ -182,6 +182,30 @@ def run(ctx, max_step, stop_time):
     return r
 
 
+def paper_options(settings):
+    """ecg_paper_options from the euler.bdltv20_paper_* settings of a run
+    (core/run_config.hpp:33-52: dt -1 = eq79 CFL mode, epsilon 1, 4096 steps)."""
+    mode = settings.bdltv20_paper_t1_s2
+    if mode not in abi.PAPER_MODE:
+        raise ValueError("Unsupported euler.bdltv20_paper_t1_s2 setting.")
+    o = abi.PaperOptions()
+    o.mode = abi.PAPER_MODE[mode]
+    o.fixed_dt = float(settings.extra.get("bdltv20_paper_t1_s2_dt", -1.0))
+    o.epsilon = float(settings.extra.get("bdltv20_paper_epsilon", 1.0))
+    o.max_steps = int(settings.extra.get("bdltv20_paper_t1_s2_max_steps", 4096))
+    return o
+
+
+def run_bdltv20_paper_t1_s2(ctx, settings):
+    """run_bdltv20_paper_t1_s2 (imex/imex_bdltv20_direct_driver.hpp:44-779) on the
+    device: initialises the context from its problem, runs the direct T1/S2
+    driver, and returns its report (abi.PaperResult)."""
+    o = paper_options(settings)
+    r = abi.PaperResult()
+    check(load().ecg_paper_t1s2_run(ctx.handle, C.byref(o), C.byref(r)), "run_bdltv20_paper_t1_s2", ctx.handle)
+    return r
+
+
 class Batch:
     """Many independent explicit solves of uneven grid sizes advanced together
     (ecg_batch_*): one persistent launch per step for the whole batch, CUDA
@@ -258,5 +282,6 @@ __all__ = [
     "initialize_state",
     "read_config",
     "run",
+    "run_bdltv20_paper_t1_s2",
     "solver_status_str",
 ]

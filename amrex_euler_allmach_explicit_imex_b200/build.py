@@ -37,6 +37,7 @@ SOURCES = {
     "batched.cu": ["-fmad=true"],
     "adjoint.cu": ["-fmad=true"],
     "noalloc.cu": [],
+    "paper.cu": ["-fmad=false"],
 }
 
 

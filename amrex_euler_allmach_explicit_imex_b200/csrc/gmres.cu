@@ -133,7 +133,9 @@ __device__ __forceinline__ int pmap(int k, int n, int per)
 
 // Row r of A v with A the source-map pressure operator
 // (imex_source_map_helpers.hpp:533-543); columns at a fixed Dirichlet
-// pressure are not part of A (their terms are in the right-hand side).
+// pressure are not part of A (their terms are in the right-hand side): the
+// bubble's left boundary, and with op.drop every column outside a
+// non-periodic axis (the direct T1/S2 driver, imex_bdltv20_direct_driver.hpp:455-466).
 template <typename T>
 __device__ __forceinline__ T apply_row(const EcgPressureOp& op, const T* __restrict__ v, int i, int j, long long r)
 {
@@ -146,11 +148,16 @@ __device__ __forceinline__ T apply_row(const EcgPressureOp& op, const T* __restr
   const long long row = static_cast<long long>(j) * nx;
   T acc = (static_cast<T>(op.diag0) + xc * (he + hw) + yc * (hn + hs)) * __ldcg(v + r);
   const bool fix = op.bubble && !op.px;
+  const bool dropx = op.drop && !op.px, dropy = op.drop && !op.py;
   auto vx = [&](int ci) -> T {
     if (fix && ci < 0) return T(0);
+    if (dropx && (ci < 0 || ci >= nx)) return T(0);
     return __ldcg(v + row + pmap(ci, nx, op.px));
   };
-  auto vy = [&](int cj) -> T { return __ldcg(v + static_cast<long long>(pmap(cj, ny, op.py)) * nx + i); };
+  auto vy = [&](int cj) -> T {
+    if (dropy && (cj < 0 || cj >= ny)) return T(0);
+    return __ldcg(v + static_cast<long long>(pmap(cj, ny, op.py)) * nx + i);
+  };
   acc += -xc * he * vx(i + 2) - xc * (he - hw) * vx(i + 1) + xc * (he - hw) * vx(i - 1) - xc * hw * vx(i - 2);
   acc += -yc * hn * vy(j + 2) - yc * (hn - hs) * vy(j + 1) + yc * (hn - hs) * vy(j - 1) - yc * hs * vy(j - 2);
   return acc;

@@ -72,7 +72,8 @@ extern const EcgImexOps ecg_imex_fast_ops;
 // Matrix-free pressure operator of source_map_pressure_row_data
 // (imex_source_map_helpers.hpp:533-543) from the face enthalpies.
 struct EcgPressureOp {
-  int nx, ny, px, py, bubble, pad;
+  int nx, ny, px, py, bubble;
+  int drop;          // columns outside a non-periodic axis are not in A (their terms are in the rhs)
   double diag0;      // 1 / (gamma - 1)
   double xc, yc;     // dt^2 / (4 dx^2), dt^2 / (4 dy^2)
   const double* hx;  // (nx+1) x ny

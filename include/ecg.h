@@ -267,6 +267,49 @@ typedef struct ecg_run_result {
   ecg_diagnostics diagnostics;  /* after the last step */
 } ecg_run_result;
 
+/* Direct BDLTV20 T1/S2 driver (imex/imex_bdltv20_direct_driver.hpp:44-779):
+ * the euler.bdltv20_paper_t1_s2 settings of RunConfig (core/run_config.hpp:33-52). */
+typedef enum ecg_paper_mode {
+  ECG_PAPER_OFF = 0,
+  ECG_PAPER_TORO_X_EXACT_DIRICHLET_Y_PERIODIC = 1, /* "toro_x_exact_dirichlet_y_periodic_2d" */
+  ECG_PAPER_TORO_XY_EXACT_DIRICHLET = 2,           /* "toro_xy_exact_dirichlet_2d" */
+  ECG_PAPER_GRESHO_EXACT_DIRICHLET = 3,            /* "gresho_exact_dirichlet_2d" */
+  ECG_PAPER_ISENTROPIC_VORTEX_PERIODIC = 4,        /* "isentropic_vortex_periodic_2d" */
+  ECG_PAPER_ADVECTION_BLOB_PERIODIC = 5            /* "advection_blob_periodic_2d" */
+} ecg_paper_mode;
+
+typedef struct ecg_paper_options {
+  int32_t mode;        /* ecg_paper_mode */
+  int32_t max_steps;   /* bdltv20_paper_t1_s2_max_steps */
+  double epsilon;      /* bdltv20_paper_epsilon */
+  double fixed_dt;     /* bdltv20_paper_t1_s2_dt: > 0 fixed, < 0 eq79 CFL mode */
+} ecg_paper_options;
+
+/* The key=value report of run_bdltv20_paper_t1_s2 (:686-777), numeric fields. */
+typedef struct ecg_paper_result {
+  int32_t steps;
+  int32_t solver_failure_count;
+  int32_t gmres_iterations_max;
+  int32_t enthalpy_guard_count;
+  int32_t nonfinite_count;
+  int32_t nonpositive_count;
+  int32_t passed;                 /* bdltv20_paper_t1_s2_status == passed */
+  int32_t pad;
+  double final_time;
+  double pressure_residual_linf_max;
+  double pressure_relative_residual_linf_max;
+  double rho_min;
+  double pressure_min;
+  double density_l1_error;
+  double velocity_l1_error;
+  double pressure_l1_error;
+  double density_l2_error;
+  double velocity_l2_error;
+  double pressure_l2_error;
+  double density_linf_error;
+  double pressure_linf_error;
+} ecg_paper_result;
+
 /* Failure categories of the driver loop (driver_main.hpp:216-340). */
 enum {
   ECG_FAILURE_NONE = 0,
@@ -349,6 +392,13 @@ ecg_status ecg_imex_step(ecg_ctx* ctx, double dt, ecg_imex_diag* out);
  * dt, step and fail-fast diagnostics per step, no host round trip for the
  * explicit method. */
 ecg_status ecg_run(ecg_ctx* ctx, int32_t max_step, double stop_time, ecg_run_result* out);
+/* run_bdltv20_paper_t1_s2 (imex/imex_bdltv20_direct_driver.hpp:44-779): the
+ * direct T1/S2 driver of the report rows, on the device.  It initialises the
+ * context's state from the configured problem (ε-scaled energy), steps to
+ * stop_time or opts->max_steps, and leaves the final (ε-scaled) state in the
+ * context.  The configuration must satisfy the reference's checks for the
+ * mode (core/config_reader.hpp:133-258), else ECG_ERR_BAD_ARG. */
+ecg_status ecg_paper_t1s2_run(ecg_ctx* ctx, const ecg_paper_options* opts, ecg_paper_result* out);
 
 /* ---- adjoint of the explicit step --------------------------------------- */
 /* Vector-Jacobian product of U1 = euler_fv_one_step(U0; dt) with dt held

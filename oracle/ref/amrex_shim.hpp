@@ -21,6 +21,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <limits>
 #include <map>
@@ -67,11 +68,60 @@ inline const T& max(const T& a, const T& b, const Ts&... c) noexcept { return ma
 
 [[noreturn]] inline void Abort(const std::string& msg) { throw std::runtime_error(msg); }
 
-// Print: output is discarded (the oracle compares numbers, not text).
-// iostreams are kept out of every path the oracle calls.
+// Print: output is discarded unless a caller collects it (print_sink()),
+// with doubles written as %.17g (the precision the reference's driver
+// reports at) and stream manipulators ignored.  iostreams are kept out of
+// every path the oracle calls.
+inline std::string*& print_sink()
+{
+  static std::string* sink = nullptr;
+  return sink;
+}
 struct Print {
   template <class T>
   Print& operator<<(const T&) { return *this; }
+  Print& operator<<(const char* s)
+  {
+    if (print_sink()) print_sink()->append(s);
+    return *this;
+  }
+  Print& operator<<(const std::string& s)
+  {
+    if (print_sink()) print_sink()->append(s);
+    return *this;
+  }
+  Print& operator<<(char c)
+  {
+    if (print_sink()) print_sink()->push_back(c);
+    return *this;
+  }
+  Print& operator<<(double v) { return num("%.17g", v); }
+  Print& operator<<(float v) { return num("%.17g", static_cast<double>(v)); }
+  Print& operator<<(int v) { return inum(v); }
+  Print& operator<<(long v) { return inum(v); }
+  Print& operator<<(long long v) { return inum(v); }
+  Print& operator<<(unsigned v) { return inum(static_cast<long long>(v)); }
+  Print& operator<<(bool v) { return inum(v ? 1 : 0); }
+
+ private:
+  Print& num(const char* fmt, double v)
+  {
+    if (print_sink()) {
+      char b[64];
+      std::snprintf(b, sizeof(b), fmt, v);
+      print_sink()->append(b);
+    }
+    return *this;
+  }
+  Print& inum(long long v)
+  {
+    if (print_sink()) {
+      char b[32];
+      std::snprintf(b, sizeof(b), "%lld", v);
+      print_sink()->append(b);
+    }
+    return *this;
+  }
 };
 
 struct Dim3 { int x, y, z; };

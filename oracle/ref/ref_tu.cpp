@@ -466,4 +466,18 @@ double ecref_gresho_density_l1(const double* u)
   return compute_gresho_metrics(s, f.geom, g_cfg).density_l1_error;
 }
 
+// run_bdltv20_paper_t1_s2 (imex/imex_bdltv20_direct_driver.hpp:44-779), the
+// reference's direct T1/S2 driver, on the configured run: returns its exit
+// code and writes its key=value report (at most len bytes) into out.
+int ecref_paper_run(char* out, int len)
+{
+  if (!g_have_cfg) return -1;
+  std::string text;
+  amrex::print_sink() = &text;
+  const int rc = run_bdltv20_paper_t1_s2(g_cfg);
+  amrex::print_sink() = nullptr;
+  if (out && len > 0) std::snprintf(out, static_cast<size_t>(len), "%s", text.c_str());
+  return rc;
+}
+
 }  // extern "C"

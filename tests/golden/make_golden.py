@@ -8,6 +8,7 @@ single-box AMReX shim):
 
 Every number in the fixtures is the reference's output on seeded inputs.
 """
+import json
 import os
 import sys
 
@@ -184,11 +185,63 @@ def imex_cases(r):
     return out
 
 
+PAPER_BASE = {"euler.method": "imex", "euler.spatial_order": 2, "euler.imex_acoustic_startup": 0,
+              "euler.imex_picard_iterations": 2, "euler.imex_solver_tol": "1e-10", "euler.imex_solver_max_iter": 120}
+PAPER_CASES = {
+    "toro_x": dict(PAPER_BASE, **{"euler.bdltv20_paper_t1_s2": "toro_x_exact_dirichlet_y_periodic_2d",
+                                  "euler.problem": "toro1", "euler.field_boundary": "exact_dirichlet",
+                                  "geometry.is_periodic": "0 1", "amr.n_cell": "64 4", "geometry.prob_hi": "1 0.0625",
+                                  "euler.bdltv20_paper_t1_s2_dt": 0.002, "stop_time": 0.01}),
+    "toro_xy": dict(PAPER_BASE, **{"euler.bdltv20_paper_t1_s2": "toro_xy_exact_dirichlet_2d", "euler.problem": "toro1",
+                                   "euler.field_boundary": "exact_dirichlet", "geometry.is_periodic": "0 0",
+                                   "amr.n_cell": "48 4", "geometry.prob_hi": "1 0.08333333333333333", "prob.test": 2,
+                                   "euler.bdltv20_paper_t1_s2_dt": 0.002, "stop_time": 0.008}),
+    "gresho": dict(PAPER_BASE, **{"euler.bdltv20_paper_t1_s2": "gresho_exact_dirichlet_2d",
+                                  "euler.problem": "gresho_vortex", "euler.field_boundary": "exact_dirichlet",
+                                  "geometry.is_periodic": "0 0", "amr.n_cell": "24 24", "geometry.prob_lo": "-0.5 -0.5",
+                                  "geometry.prob_hi": "0.5 0.5", "euler.mach": 0.1, "euler.pressure": 1 / (1.4 * 0.01),
+                                  "euler.imex_cfl": 0.4, "euler.bdltv20_paper_t1_s2_max_steps": 4, "stop_time": 0.05}),
+    "gresho_eps": dict(PAPER_BASE, **{"euler.bdltv20_paper_t1_s2": "gresho_exact_dirichlet_2d",
+                                      "euler.problem": "gresho_vortex", "euler.field_boundary": "exact_dirichlet",
+                                      "geometry.is_periodic": "0 0", "amr.n_cell": "20 20",
+                                      "geometry.prob_lo": "-0.5 -0.5", "geometry.prob_hi": "0.5 0.5",
+                                      "euler.mach": 0.1, "euler.pressure": 1 / (1.4 * 0.01),
+                                      "euler.bdltv20_paper_epsilon": 0.5, "euler.imex_cfl": 0.4,
+                                      "euler.bdltv20_paper_t1_s2_max_steps": 3, "stop_time": 0.05}),
+    "vortex": dict(PAPER_BASE, **{"euler.bdltv20_paper_t1_s2": "isentropic_vortex_periodic_2d",
+                                  "euler.problem": "isentropic_vortex", "geometry.is_periodic": "1 1",
+                                  "amr.n_cell": "24 24", "geometry.prob_lo": "-5 -5", "geometry.prob_hi": "5 5",
+                                  "euler.vortex_center": "0 0", "euler.velocity": "1 1", "euler.imex_cfl": 0.4,
+                                  "euler.bdltv20_paper_t1_s2_max_steps": 3, "stop_time": 1.0}),
+    "blob": dict(PAPER_BASE, **{"euler.bdltv20_paper_t1_s2": "advection_blob_periodic_2d",
+                                "euler.problem": "advection_blob", "geometry.is_periodic": "1 1", "amr.n_cell": "24 24",
+                                "euler.imex_cfl": 0.4, "euler.bdltv20_paper_t1_s2_max_steps": 3, "stop_time": 0.05}),
+}
+
+
+def paper_cases(r):
+    """The reference's direct T1/S2 driver (imex_bdltv20_direct_driver.hpp:44-779)
+    on small runs of every mode: its exit code and key=value report."""
+    out = {}
+    for name, kv in PAPER_CASES.items():
+        r.configure(kv)
+        rc, rep = r.paper_run()
+        out[name] = {"kv": kv_text(kv), "rc": rc, "report": rep}
+    return out
+
+
 def main():
     r = RefOracle()
-    np.savez_compressed(os.path.join(HERE, "explicit_cases.npz"), **explicit_cases(r))
-    np.savez_compressed(os.path.join(HERE, "sod_400x4.npz"), **sod_case(r))
-    np.savez_compressed(os.path.join(HERE, "imex_cases.npz"), **imex_cases(r))
+    only = sys.argv[1:]
+    if not only or "explicit" in only:
+        np.savez_compressed(os.path.join(HERE, "explicit_cases.npz"), **explicit_cases(r))
+    if not only or "sod" in only:
+        np.savez_compressed(os.path.join(HERE, "sod_400x4.npz"), **sod_case(r))
+    if not only or "imex" in only:
+        np.savez_compressed(os.path.join(HERE, "imex_cases.npz"), **imex_cases(r))
+    if not only or "paper" in only:
+        with open(os.path.join(HERE, "paper_cases.json"), "w") as f:
+            json.dump(paper_cases(r), f, indent=1, sort_keys=True)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -176,6 +176,8 @@ class RefOracle:
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference is available")
         lib = C.CDLL(path)
+        lib.ecref_paper_run.argtypes = [C.c_char_p, C.c_int]
+        lib.ecref_paper_run.restype = C.c_int
         lib.ecref_configure.argtypes = [C.c_char_p]
         lib.ecref_last_error.restype = C.c_char_p
         lib.ecref_get_config.argtypes = [_CFG]
@@ -207,6 +209,17 @@ class RefOracle:
         self.lib.ecref_get_config(C.byref(c))
         self.cfg = c
         return c
+
+    def paper_run(self):
+        """The reference's direct T1/S2 driver on the configured run: (exit
+        code, {key: value} of its report)."""
+        buf = C.create_string_buffer(1 << 16)
+        rc = self.lib.ecref_paper_run(buf, len(buf))
+        rep = {}
+        for line in buf.value.decode().splitlines():
+            k, _, v = line.partition("=")
+            rep[k.strip()] = v.strip()
+        return rc, rep
 
     def initialize(self):
         u = _state(self.cfg)

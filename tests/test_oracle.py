@@ -153,3 +153,32 @@ def test_oracle_mach122_configuration(oracle):
     assert np.array_equal(gh[2, 1, 2:-2], -w[2, 0]) and np.array_equal(gh[2, 0, 2:-2], -w[2, 1])
     assert np.array_equal(gh[2, -2, 2:-2], -w[2, -1]) and np.array_equal(gh[2, -1, 2:-2], -w[2, -2])
     assert np.array_equal(gh[0, 2:-2, 0], np.full(16, rho2))      # inflow column
+
+
+def test_paper_fixture_covers_every_mode():
+    """tests/golden/paper_cases.json: one reference run per direct-driver mode."""
+    import json
+    import os
+
+    with open(os.path.join(os.path.dirname(__file__), "golden", "paper_cases.json")) as f:
+        cases = json.load(f)
+    modes = {c["report"]["bdltv20_paper_t1_s2"] for c in cases.values()}
+    assert modes == set(abi.PAPER_MODE) - {"off"}
+    for c in cases.values():
+        s = read_config(c["kv"])
+        assert s.bdltv20_paper_t1_s2 == c["report"]["bdltv20_paper_t1_s2"]
+        assert int(c["report"]["bdltv20_paper_steps"]) >= 3
+
+
+def test_paper_fixture_reproduces_live_reference(ref):
+    """The reference driver, run again here, prints the committed report."""
+    import json
+    import os
+
+    with open(os.path.join(os.path.dirname(__file__), "golden", "paper_cases.json")) as f:
+        cases = json.load(f)
+    for name in ("toro_xy", "gresho_eps", "vortex"):
+        ref.configure(cases[name]["kv"])
+        rc, rep = ref.paper_run()
+        assert rc == cases[name]["rc"]
+        assert rep == cases[name]["report"], name
