@@ -20,9 +20,13 @@
 //    pass only when ||w'|| < ||w|| / sqrt(2)), with all dot products of a pass
 //    fused into one sweep and one grid reduction;
 //  * the iterate is formed once, at the end.
-// Mixed precision: FP32 basis, FP32 operator, FP64-accumulated dot products
-// inside FP64 iterative refinement on the true FP64 residual; the stopping
-// test stays the reference's on the FP64 residual.
+// Mixed precision: the Krylov basis is stored in FP32 (half the bytes of
+// every sweep over it); the operator, w, the dot products, the Hessenberg
+// column, the rotations and the residual recurrence stay FP64, so the basis
+// rounding is the only FP32 error (a compressed-basis GMRES).  The solve
+// restarts from the current iterate whenever the recurrence says the cycle
+// converged or its residual fell by inner_rtol, and every cycle opens with the
+// true FP64 residual b - A x: the reference's stopping rule is applied to it.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -54,16 +58,12 @@ struct GmresArgs {
   const double* b;
   const double* x0;
   double* x;
-  double* V;     // (m+1) x n
+  double* V;     // (m+1) x n (FP64 solve)
   double* w;     // n
-  double* r;     // n
+  double* r;     // n: residual recurrence
   float* V32;    // (m+1) x n (mixed)
-  float* w32;
-  float* r32;    // inner right-hand side
   double* part;  // nblocks x ld
-  double* red;   // ld reduced values
   double* R;     // column-major (m+1) x m
-  double* yv;    // m
   GridBar* bar;
   EcgGmresResult* res;
   int ld;
@@ -71,37 +71,36 @@ struct GmresArgs {
   int max_iter;
   double tol;
   int mixed;
-  int inner_max;
-  double inner_rtol;
-  int max_refine;
+  int inner_max;      // mixed: iterations per cycle
+  double inner_rtol;  // mixed: restart when the recurrence residual fell by this factor
+  int max_refine;     // mixed: cycles
   long long spin_limit;
 };
 
 __device__ __forceinline__ unsigned int ld_volatile(const unsigned int* p) { return *reinterpret_cast<const volatile unsigned int*>(p); }
 __device__ __forceinline__ int ld_volatile_i(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
 
-// Grid-wide barrier over co-resident blocks (cooperative launch), with a
-// bounded spin: a block that waits longer than spin_limit polls sets the
-// timeout flag and leaves; every block then exits at its next check.
+// Grid-wide barrier over co-resident blocks (cooperative launch): one
+// arrival counter that only grows (zeroed by the host before the launch), so
+// barrier number g is passed once it reaches (g + 1) x blocks; one atomic per
+// block and no reset on the critical path.  The spin is bounded: a block that
+// waits longer than spin_limit polls sets the timeout flag and leaves; every
+// block then exits at its next check.
 __device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned int& gen, long long spin_limit)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int g = gen;
+    const unsigned int target = (gen + 1u) * gridDim.x;
     __threadfence();
-    const unsigned int t = atomicAdd(&bar->arrive, 1u);
-    if (t == gridDim.x - 1) {
-      atomicExch(&bar->arrive, 0u);
-      __threadfence();
-      atomicExch(&bar->gen, g + 1u);
-    } else {
+    const unsigned int t = atomicAdd(&bar->arrive, 1u) + 1u;
+    if (t != target) {
       long long spins = 0;
-      while (ld_volatile(&bar->gen) == g) {
+      while (static_cast<int>(ld_volatile(&bar->arrive) - target) < 0) {
         if (++spins > spin_limit) {
           atomicExch(&bar->timeout, 1);
           break;
         }
-        __nanosleep(40);
+        __nanosleep(32);
       }
     }
     __threadfence();
@@ -111,15 +110,14 @@ __device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned int& gen, long 
   return ld_volatile_i(&bar->timeout) == 0;
 }
 
-__device__ __forceinline__ int wrapi(int i, int n)
-{
-  int r = i % n;
-  return r < 0 ? r + n : r;
-}
-// source_map_index: wrap or even reflection (imex_source_map_helpers.hpp:169-188)
+// source_map_index: wrap or even reflection (imex_source_map_helpers.hpp:169-188),
+// for k within two cells of [0, n)
 __device__ __forceinline__ int pmap(int k, int n, int per)
 {
-  if (per) return wrapi(k, n);
+  if (per) {
+    if (n >= 2) return k < 0 ? k + n : (k >= n ? k - n : k);
+    return 0;
+  }
   if (k < 0) {
     const int r = -k - 1;
     return r < n - 1 ? r : n - 1;
@@ -131,56 +129,112 @@ __device__ __forceinline__ int pmap(int k, int n, int per)
   return k;
 }
 
-// Row r of A v with A the source-map pressure operator
-// (imex_source_map_helpers.hpp:533-543); columns at a fixed Dirichlet
-// pressure are not part of A (their terms are in the right-hand side): the
-// bubble's left boundary, and with op.drop every column outside a
-// non-periodic axis (the direct T1/S2 driver, imex_bdltv20_direct_driver.hpp:455-466).
-template <typename T>
-__device__ __forceinline__ T apply_row(const EcgPressureOp& op, const T* __restrict__ v, int i, int j, long long r)
+template <typename TV>
+__device__ __forceinline__ double ldv(const TV* p)
+{
+  return static_cast<double>(__ldcg(p));
+}
+
+// acc[r] + sgn sum_{i<cnt} c[i] V_i[q_r] for R rows at once, i ascending (the
+// rounding of the plain loop), with 32 (FP64) or 16 (FP32) loads of the basis in flight before
+// the first FMA (the stores that follow a call would otherwise keep the
+// compiler from starting the next row's loads: the new basis vector aliases V).
+template <typename TV, bool SUB, int R>
+__device__ __forceinline__ void basis_combine(double (&acc)[R], const TV* __restrict__ V, long long n, const int (&q)[R],
+                                              const double* c, int cnt)
+{
+  constexpr int B = (sizeof(TV) == 8 ? 32 : 16) / R;
+  for (int i0 = 0; i0 < cnt; i0 += B) {
+    TV a[R][B];
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+#pragma unroll
+      for (int r = 0; r < R; ++r) a[r][k] = i0 + k < cnt ? __ldcg(V + static_cast<long long>(i0 + k) * n + q[r]) : TV(0);
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+      if (i0 + k < cnt) {
+        const double ck = c[i0 + k];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          acc[r] = SUB ? acc[r] - ck * static_cast<double>(a[r][k]) : acc[r] + ck * static_cast<double>(a[r][k]);
+      }
+  }
+}
+
+// Rows q_r = j nx + i of A v with A the source-map pressure operator
+// (imex_source_map_helpers.hpp:533-543), in FP64 whatever the storage of v,
+// R rows with every load issued before the arithmetic (indices are always in
+// range; left-out terms are selected away after the load).  Columns at a
+// fixed Dirichlet pressure are not part of A (their terms are in the
+// right-hand side): the bubble's left boundary, and with op.drop every column
+// outside a non-periodic axis (the direct T1/S2 driver,
+// imex_bdltv20_direct_driver.hpp:455-466).
+template <typename TV, int R>
+__device__ __forceinline__ void apply_rows(const EcgPressureOp& op, const TV* __restrict__ v, const int (&q)[R],
+                                           double (&out)[R])
 {
   const int nx = op.nx, ny = op.ny;
-  const T he = static_cast<T>(op.hx[static_cast<long long>(j) * (nx + 1) + i + 1]);
-  const T hw = static_cast<T>(op.hx[static_cast<long long>(j) * (nx + 1) + i]);
-  const T hn = static_cast<T>(op.hy[static_cast<long long>(j + 1) * nx + i]);
-  const T hs = static_cast<T>(op.hy[static_cast<long long>(j) * nx + i]);
-  const T xc = static_cast<T>(op.xc), yc = static_cast<T>(op.yc);
-  const long long row = static_cast<long long>(j) * nx;
-  T acc = (static_cast<T>(op.diag0) + xc * (he + hw) + yc * (hn + hs)) * __ldcg(v + r);
+  const double* __restrict__ hx = op.hx;
+  const double* __restrict__ hy = op.hy;
   const bool fix = op.bubble && !op.px;
   const bool dropx = op.drop && !op.px, dropy = op.drop && !op.py;
-  auto vx = [&](int ci) -> T {
-    if (fix && ci < 0) return T(0);
-    if (dropx && (ci < 0 || ci >= nx)) return T(0);
-    return __ldcg(v + row + pmap(ci, nx, op.px));
-  };
-  auto vy = [&](int cj) -> T {
-    if (dropy && (cj < 0 || cj >= ny)) return T(0);
-    return __ldcg(v + static_cast<long long>(pmap(cj, ny, op.py)) * nx + i);
-  };
-  acc += -xc * he * vx(i + 2) - xc * (he - hw) * vx(i + 1) + xc * (he - hw) * vx(i - 1) - xc * hw * vx(i - 2);
-  acc += -yc * hn * vy(j + 2) - yc * (hn - hs) * vy(j + 1) + yc * (hn - hs) * vy(j - 1) - yc * hs * vy(j - 2);
-  return acc;
+  double h[R][4], c[R][9];
+  bool keep[R][8];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = q[r] / nx, i = q[r] - j * nx;
+    h[r][0] = hx[j * (nx + 1) + i + 1];
+    h[r][1] = hx[j * (nx + 1) + i];
+    h[r][2] = hy[(j + 1) * nx + i];
+    h[r][3] = hy[j * nx + i];
+    c[r][0] = ldv(v + q[r]);
+    const int row = j * nx;
+    const int dx[4] = {2, 1, -1, -2};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int ci = i + dx[k], cj = j + dx[k];
+      keep[r][k] = !((fix && ci < 0) || (dropx && (ci < 0 || ci >= nx)));
+      keep[r][4 + k] = !(dropy && (cj < 0 || cj >= ny));
+      c[r][1 + k] = ldv(v + row + pmap(ci, nx, op.px));
+      c[r][5 + k] = ldv(v + pmap(cj, ny, op.py) * nx + i);
+    }
+  }
+  const double xc = op.xc, yc = op.yc;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const double he = h[r][0], hw = h[r][1], hn = h[r][2], hs = h[r][3];
+    double e[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) e[k] = keep[r][k] ? c[r][1 + k] : 0.0;
+    double acc = (op.diag0 + xc * (he + hw) + yc * (hn + hs)) * c[r][0];
+    acc += -xc * he * e[0] - xc * (he - hw) * e[1] + xc * (he - hw) * e[2] - xc * hw * e[3];
+    acc += -yc * hn * e[4] - yc * (hn - hs) * e[5] + yc * (hn - hs) * e[6] - yc * hs * e[7];
+    out[r] = acc;
+  }
 }
 
 struct Rows {
-  long long r0, r1;
+  int r0, r1;
 };
 __device__ __forceinline__ Rows own_rows(long long n)
 {
   const long long per = (n + gridDim.x - 1) / gridDim.x;
-  Rows o;
-  o.r0 = per * blockIdx.x;
-  o.r1 = o.r0 + per < n ? o.r0 + per : n;
-  if (o.r0 > n) o.r0 = n;
-  return o;
+  long long r0 = per * blockIdx.x, r1 = r0 + per;
+  if (r1 > n) r1 = n;
+  if (r0 > n) r0 = n;
+  return Rows{static_cast<int>(r0), static_cast<int>(r1)};
 }
 
 // Shared-memory layout of one block (doubles): six vectors of m+8 (Givens
 // cosines/sines, rotated rhs g, current Hessenberg column, reduced values,
-// update coefficients), per-warp partials of one sum (NW), and NT + m + 8
-// scratch (grid reductions stage at most max(NT, m + 8) values).
+// update coefficients), per-warp partials of one sum (NW), NT + m + 8 scratch
+// (grid reductions stage at most max(NT, m + 8) values), and the per-warp
+// partials of every dot product of a sweep (NW x LW).
 constexpr int NW = NT / 32;
+// dot products a thread accumulates per pass over its rows (16 spills under
+// the 128-register cap of 512-thread blocks)
+constexpr int DG_ROWS = 8;
+__host__ __device__ constexpr int dots_ld(int m) { return ((m + 3 + DG_ROWS - 1) / DG_ROWS) * DG_ROWS; }
 struct Smem {
   double* cs;
   double* sn;
@@ -190,6 +244,7 @@ struct Smem {
   double* coef;
   double* wpart;
   double* scratch;
+  double* dpart;
 };
 __device__ __forceinline__ Smem carve(double* base, int m)
 {
@@ -203,9 +258,13 @@ __device__ __forceinline__ Smem carve(double* base, int m)
   s.coef = s.red + L;
   s.wpart = s.coef + L;
   s.scratch = s.wpart + NW;
+  s.dpart = s.scratch + NT + L;
   return s;
 }
-inline size_t smem_bytes(int m) { return sizeof(double) * (static_cast<size_t>(7) * (m + 8) + NW + NT); }
+inline size_t smem_bytes(int m)
+{
+  return sizeof(double) * (static_cast<size_t>(7) * (m + 8) + NW + NT + static_cast<size_t>(NW) * dots_ld(m));
+}
 
 // Per-thread value v of one sum -> per-warp partial (lane 0 stores).
 __device__ __forceinline__ void warp_partial(double v, double* wpart)
@@ -239,7 +298,14 @@ __device__ __forceinline__ void grid_reduce_redundant(const double* part, int ld
     const int q = t % cnt, gi = t / cnt;
     const int b0 = gi * per, b1 = b0 + per < nb ? b0 + per : nb;
     double s = 0.0;
-    for (int b = b0; b < b1; ++b) s += __ldcg(part + static_cast<long long>(b) * ld + q);
+    for (int c0 = b0; c0 < b1; c0 += 16) {  // 16 loads in flight, summed in block order
+      double t[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) t[k] = c0 + k < b1 ? __ldcg(part + static_cast<long long>(c0 + k) * ld + q) : 0.0;
+#pragma unroll
+      for (int k = 0; k < 16; ++k)
+        if (c0 + k < b1) s += t[k];
+    }
     if (cnt * groups <= NT) scratch[gi * cnt + q] = s;
     else scratch[q] = s;  // cnt > NT: one group
   }
@@ -253,6 +319,17 @@ __device__ __forceinline__ void grid_reduce_redundant(const double* part, int ld
     out[q] = s;
   }
   __syncthreads();
+}
+
+// sum_{q<k} red[q]^2 by every warp (lanes stride, fixed shuffle tree): the
+// same value in every thread of every block.
+__device__ __forceinline__ double sum_squares(const double* red, int k)
+{
+  double s = 0.0;
+  for (int q = threadIdx.x & 31; q < k; q += 32) s += red[q] * red[q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
 }
 
 __device__ __forceinline__ double nanmax(double m, double v) { return (m < v || v != v) ? v : m; }
@@ -296,7 +373,9 @@ struct SolveState {
   int it;          // iterations completed
   int best_it;     // index of the iterate returned
   double best_linf;
+  double r0_linf;  // infinity norm of b - A x0
   int converged, breakdown, nonfinite, timeout;
+  int restart;     // mixed: the recurrence residual fell by inner_rtol
 };
 
 // Back substitution R y = g (k x k; R column-major, leading dimension ldr) by
@@ -316,66 +395,235 @@ __device__ void back_substitute(const double* R, int ldr, const double* g, int k
   __syncthreads();
 }
 
-// Dot products of the block's rows: part_row[i] = v_i . w for i < nvec, by
-// warps (warp k takes i = k, k + NW, ...), lanes striding the rows: every
-// load of a warp is coalesced and independent.  Also ||w||^2 -> part_row[nvec]
-// and a nonfinite flag of w -> part_row[nvec + 1] (when with_norm).
-template <typename T>
-__device__ __forceinline__ void block_dots(const T* __restrict__ V, long long n, const T* __restrict__ w, Rows rw,
-                                           int nvec, bool with_norm, double* part_row)
+// Warp sums of DG values by a reduce-scatter butterfly: after it, lane
+// (32 / DG) k holds the warp's sum of s[k] (DG - 1 + log2(32 / DG) shuffles in
+// place of 5 DG).  Fixed pairing: the same result in every warp and launch.
+template <int DG>
+__device__ __forceinline__ double warp_reduce_scatter(double (&s)[DG], int lane)
 {
+#pragma unroll
+  for (int h = DG / 2, off = 16; h >= 1; h >>= 1, off >>= 1) {
+    const bool up = (lane & off) != 0;
+#pragma unroll
+    for (int k = 0; k < h; ++k) {
+      const double send = up ? s[k] : s[k + h];
+      const double keep = up ? s[k + h] : s[k];
+      s[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  double v = s[0];
+#pragma unroll
+  for (int off = 16 / DG; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// Dot products of the block's rows: part_row[i] = v_i . w for i < nvec, and
+// with_norm: ||w||^2 -> part_row[nvec], a nonfinite count of w ->
+// part_row[nvec + 1].  Every thread takes part: DG sums a pass over its rows
+// (w read once a pass), a reduce-scatter of the DG sums in each warp, then
+// the warps' partials summed in warp order.
+template <typename TV>
+__device__ __forceinline__ void block_dots(const TV* __restrict__ V, long long n, const double* __restrict__ w, Rows rw,
+                                           int nvec, bool with_norm, double* part_row, double* dpart)
+{
+  constexpr int DG = DG_ROWS;
+  constexpr int SMALL = 16;  // rows a lane holds in the small-block layout
   __syncthreads();  // w of the block's rows is complete
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tot = nvec + (with_norm ? 2 : 0);
-  for (int i = warp; i < tot; i += NW) {
-    double s = 0.0;
-    if (i < nvec) {
-      // 8 rows a lane per pass, all loads issued before the first use
-      const T* vi = V + static_cast<long long>(i) * n;
-      for (long long base = rw.r0 + lane; base < rw.r1; base += 32 * 8) {
-        T a[8], b[8];
+  if (rw.r1 - rw.r0 <= 32 * SMALL) {
+    // Few rows (an L2-resident system): warp k takes vectors k, k + NW, ...
+    // over all the block's rows, lanes striding the rows with w in registers;
+    // one round trip a vector and no block-wide step between vectors.
+    double wr[SMALL];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const long long q = base + 32LL * k;
-          const bool ok = q < rw.r1;
-          a[k] = ok ? __ldcg(vi + q) : T(0);
-          b[k] = ok ? w[q] : T(0);
+    for (int k = 0; k < SMALL; ++k) {
+      const int q = rw.r0 + lane + 32 * k;
+      wr[k] = q < rw.r1 ? w[q] : 0.0;
+    }
+    for (int i = warp; i < tot; i += NW) {
+      double sm = 0.0;
+      if (i < nvec) {
+        TV av[SMALL];
+#pragma unroll
+        for (int k = 0; k < SMALL; ++k) {
+          const int q = rw.r0 + lane + 32 * k;
+          av[k] = q < rw.r1 ? __ldcg(V + static_cast<long long>(i) * n + q) : TV(0);
         }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) s += static_cast<double>(a[k]) * static_cast<double>(b[k]);
-      }
-    } else if (i == nvec) {
-#pragma unroll 4
-      for (long long q = rw.r0 + lane; q < rw.r1; q += 32) {
-        const double wd = static_cast<double>(__ldcg(w + q));
-        s += wd * wd;
-      }
-    } else {
-      for (long long q = rw.r0 + lane; q < rw.r1; q += 32)
-        if (!isfinite(static_cast<double>(__ldcg(w + q)))) s = 1.0;
-    }
+        for (int k = 0; k < SMALL; ++k) sm += static_cast<double>(av[k]) * wr[k];
+      } else if (i == nvec) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) part_row[i] = s;
+        for (int k = 0; k < SMALL; ++k) sm += wr[k] * wr[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < SMALL; ++k)
+          if (!isfinite(wr[k])) sm = 1.0;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sm += __shfl_xor_sync(0xffffffffu, sm, o);
+      if (lane == 0) part_row[i] = sm;
+    }
+    __syncthreads();
+    return;
+  }
+  for (int g0 = 0; g0 < tot; g0 += DG) {
+    double s[DG];
+#pragma unroll
+    for (int k = 0; k < DG; ++k) s[k] = 0.0;
+    // FP64 basis: two rows a pass (2 DG loads in flight); FP32: one (measured faster)
+    constexpr int RS = sizeof(TV) == 8 ? 2 : 1;
+    for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += RS * NT) {
+      const bool hb = RS == 2 && q + NT < rw.r1;
+      const int qb = hb ? q + NT : q;
+      const double wq[2] = {w[q], hb ? w[qb] : 0.0};
+      TV a[2][DG];
+#pragma unroll
+      for (int k = 0; k < DG; ++k) {
+        a[0][k] = g0 + k < nvec ? __ldcg(V + static_cast<long long>(g0 + k) * n + q) : TV(0);
+        a[1][k] = g0 + k < nvec && hb ? __ldcg(V + static_cast<long long>(g0 + k) * n + qb) : TV(0);
+      }
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        if (r == 1 && !hb) break;
+#pragma unroll
+        for (int k = 0; k < DG; ++k) {
+          const int i = g0 + k;
+          if (i < nvec) s[k] += static_cast<double>(a[r][k]) * wq[r];
+          else if (i == nvec && with_norm) s[k] += wq[r] * wq[r];
+          else if (i == nvec + 1 && with_norm && !isfinite(wq[r])) s[k] = 1.0;
+        }
+      }
+    }
+    const double v = warp_reduce_scatter<DG>(s, lane);
+    if ((lane & (32 / DG - 1)) == 0) dpart[(g0 + lane / (32 / DG)) * NW + warp] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < tot; i += NT) {
+    double t = 0.0;
+    for (int wv = 0; wv < NW; ++wv) t += dpart[i * NW + wv];
+    part_row[i] = t;
   }
   __syncthreads();
 }
 
-// One GMRES solve A x = b from x0 in precision T on this block's rows.
-//  reference_rule (FP64): stop at ||r_j||inf <= tol or ||r_j||inf/max(||b||inf,1)
-//    <= tol with r_j carried by the residual recurrence in rres; return the
-//    iterate with the smallest ||r||inf otherwise.  The infinity norm of r_j
-//    is reduced after the barrier that opens iteration j+1 (the barrier is
-//    needed there anyway for the SpMV of v_{j+1}).
-//  otherwise (FP32 inner solve): stop at |g_{j+1}| <= rtol * beta.
-template <typename T>
-__device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, const T* __restrict__ x0vec,
-                             T* __restrict__ xvec, T* __restrict__ V, T* __restrict__ w, double* __restrict__ rres,
-                             int kmax, double tol, double rtol, bool reference_rule, unsigned int& gen, double* shbase)
+// The row sweeps of a cycle, R rows of the block at a time (R = 2 when the
+// block has more rows than threads, else 1: no duplicate loads).
+
+// w = b - A x0 and rres = w on the block's rows; running max |b|, max |r|, sum r^2.
+template <int R>
+__device__ __forceinline__ void sweep_r0(const EcgPressureOp& op, Rows rw, const double* __restrict__ b,
+                                         const double* __restrict__ x0, double* __restrict__ w, double* __restrict__ rres,
+                                         double& bmax, double& rmax, double& r2)
+{
+  for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += R * NT) {
+    int qq[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) qq[r] = q + r * NT < rw.r1 ? q + r * NT : q;
+    double ax[R];
+    apply_rows<double, R>(op, x0, qq, ax);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (q + r * NT >= rw.r1) break;
+      const double bq = b[qq[r]];
+      const double rq = bq - ax[r];
+      bmax = nanmax(bmax, fabs(bq));
+      rmax = nanmax(rmax, fabs(rq));
+      r2 += rq * rq;
+      w[qq[r]] = rq;
+      rres[qq[r]] = rq;
+    }
+  }
+}
+
+// w = A v on the block's rows.
+template <typename TV, int R>
+__device__ __forceinline__ void sweep_spmv(const EcgPressureOp& op, Rows rw, const TV* __restrict__ v,
+                                           double* __restrict__ w)
+{
+  for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += R * NT) {
+    int qq[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) qq[r] = q + r * NT < rw.r1 ? q + r * NT : q;
+    double av[R];
+    apply_rows<TV, R>(op, v, qq, av);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (q + r * NT < rw.r1) w[qq[r]] = av[r];
+  }
+}
+
+// out = in + sgn V c (cnt basis vectors) on the block's rows.
+template <typename TV, bool SUB, int R>
+__device__ __forceinline__ void sweep_combine(Rows rw, const TV* __restrict__ V, long long n, const double* c, int cnt,
+                                              const double* in, double* out)
+{
+  for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += R * NT) {
+    int qq[R];
+    double acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      qq[r] = q + r * NT < rw.r1 ? q + r * NT : q;
+      acc[r] = in[qq[r]];
+    }
+    basis_combine<TV, SUB, R>(acc, V, n, qq, c, cnt);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (q + r * NT < rw.r1) out[qq[r]] = acc[r];
+  }
+}
+
+// w - V c -> v_{j+1} = (w - V c) inv_nn (stored as TV), and the residual
+// recurrence rres <- cr1 rres + cr2 v_{j+1}; returns the block-local max |rres|.
+template <typename TV, int R>
+__device__ __forceinline__ double sweep_next(Rows rw, const TV* __restrict__ V, long long n, const double* c, int cnt,
+                                             const double* __restrict__ w, TV* vn, double inv_nn, double cr1, double cr2,
+                                             double* __restrict__ rres)
+{
+  double rmx = 0.0;
+  for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += R * NT) {
+    int qq[R];
+    double acc[R], rp[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      qq[r] = q + r * NT < rw.r1 ? q + r * NT : q;
+      acc[r] = w[qq[r]];
+      rp[r] = rres[qq[r]];
+    }
+    basis_combine<TV, true, R>(acc, V, n, qq, c, cnt);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (q + r * NT >= rw.r1) break;
+      const TV vq = static_cast<TV>(acc[r] * inv_nn);
+      vn[qq[r]] = vq;
+      const double rq = cr1 * rp[r] + cr2 * static_cast<double>(vq);
+      rres[qq[r]] = rq;
+      rmx = nanmax(rmx, fabs(rq));
+    }
+  }
+  return rmx;
+}
+
+// One GMRES cycle A x = b from x0, basis stored as TV, arithmetic FP64.
+// Stops at ||r_j||inf <= tol or ||r_j||inf/max(||b||inf,1) <= tol (the
+// reference's rule) with r_0 = b - A x0 computed and r_j carried by the
+// residual recurrence in rres; returns the iterate with the smallest
+// ||r||inf otherwise.  The infinity norm of r_j is reduced after the barrier
+// that opens iteration j+1 (needed there anyway for the SpMV of v_{j+1}).
+// restart_rtol > 0 (mixed): also stop, with restart set, once ||r_j||inf <=
+// restart_rtol ||r_0||inf.  x0vec and xvec may be the same array (a restart):
+// each row of x is read and then written by one thread, after the last read
+// of x0 by any other row.
+template <typename TV>
+__device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec, const double* x0vec, double* xvec,
+                             TV* __restrict__ V, double* __restrict__ w,
+                             double* __restrict__ rres, int kmax, double tol, double restart_rtol, unsigned int& gen,
+                             double* shbase)
 {
   const long long n = a.n;
   const int nx = a.op.nx;
   const Rows rw = own_rows(n);
+  const bool wide = rw.r1 - rw.r0 > NT;  // two rows a thread per pass
   const int ld = a.ld;
   const int XSLOT = ld - 1;  // block max of |r_j|, read after the next barrier
   double* part_row = a.part + static_cast<long long>(blockIdx.x) * ld;
@@ -384,22 +632,15 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
   st.it = 0;
   st.best_it = 0;
   st.best_linf = __builtin_huge_val();
-  st.converged = st.breakdown = st.nonfinite = st.timeout = 0;
+  st.r0_linf = __builtin_huge_val();
+  st.converged = st.breakdown = st.nonfinite = st.timeout = st.restart = 0;
   double beta = 0.0;
 
   // ---- r0 = b - A x0: ||b||inf, ||r0||inf, ||r0||2 ----
   {
     double bmax = 0.0, rmax = 0.0, r2 = 0.0;
-    for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
-      const int i = static_cast<int>(q % nx), j = static_cast<int>(q / nx);
-      const double bq = static_cast<double>(bvec[q]);
-      const double rq = bq - static_cast<double>(apply_row<T>(a.op, x0vec, i, j, q));
-      bmax = nanmax(bmax, fabs(bq));
-      rmax = nanmax(rmax, fabs(rq));
-      r2 += rq * rq;
-      w[q] = static_cast<T>(rq);
-      if (rres) rres[q] = rq;
-    }
+    if (wide) sweep_r0<2>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
+    else sweep_r0<1>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
     block_max_partial(bmax, part_row, 0, S.scratch);
     block_max_partial(rmax, part_row, 1, S.scratch);
     warp_partial(r2, S.wpart);
@@ -414,13 +655,15 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
   grid_reduce_redundant(a.part + 2, ld, 1, S.red, S.scratch);
   beta = sqrt(S.red[0]);
   const double bn = bn_raw > 1.0 ? bn_raw : 1.0;
+  const double rtarget = restart_rtol > 0.0 ? restart_rtol * r0inf : -1.0;
   bool stop = false;
   if (!isfinite(bn_raw) || !isfinite(r0inf)) {
     st.nonfinite = 1;
     stop = true;
   } else {
     st.best_linf = r0inf;  // update_best(initial_guess, 0)
-    if (reference_rule && (r0inf <= tol || r0inf / bn <= tol)) {
+    st.r0_linf = r0inf;
+    if (r0inf <= tol || r0inf / bn <= tol) {
       st.converged = 1;
       stop = true;
     } else if (kmax <= 0) {
@@ -436,7 +679,7 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
   }
   const double btol = kEps * 100.0 * (beta > 1.0 ? beta : 1.0);
   if (!stop) {
-    for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) V[q] = static_cast<T>(static_cast<double>(w[q]) / beta);
+    for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) V[q] = static_cast<TV>(w[q] / beta);
     if (threadIdx.x == 0) S.g[0] = beta;
     __syncthreads();
   }
@@ -446,7 +689,7 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
       st.timeout = 1;
       return st;
     }
-    if (j > 0 && reference_rule) {
+    if (j > 0) {
       // update_best / convergence test of iterate j (residual r_{j-1})
       const double linf = grid_max_redundant(a.part, ld, XSLOT, S.scratch);
       if (!isfinite(linf)) {
@@ -463,19 +706,23 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
         st.best_linf = linf;
         break;
       }
+      if (linf <= rtarget) {
+        st.restart = 1;
+        st.best_it = j;
+        st.best_linf = linf;
+        break;
+      }
     }
     if (broke) {
       st.breakdown = 1;
       break;
     }
     if (j >= kmax) break;
-    const T* vj = V + static_cast<long long>(j) * n;
+    const TV* vj = V + static_cast<long long>(j) * n;
     // ---- sweep A: w = A v_j; d_i = v_i . w (i <= j); ||w||^2; nonfinite ----
-    for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
-      const int i = static_cast<int>(q % nx), jj = static_cast<int>(q / nx);
-      w[q] = apply_row<T>(a.op, vj, i, jj, q);
-    }
-    block_dots<T>(V, n, w, rw, j + 1, true, part_row);
+    if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
+    else sweep_spmv<TV, 1>(a.op, rw, vj, w);
+    block_dots<TV>(V, n, w, rw, j + 1, true, part_row, S.dpart);
     if (!grid_sync(a.bar, gen, a.spin_limit)) {
       st.timeout = 1;
       return st;
@@ -486,8 +733,7 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
       break;
     }
     double sw = S.red[j + 1];
-    double dsum = 0.0;
-    for (int q = 0; q <= j; ++q) dsum += S.red[q] * S.red[q];
+    const double dsum = sum_squares(S.red, j + 1);
     for (int q = threadIdx.x; q <= j; q += NT) {
       S.hcol[q] = S.red[q];
       S.coef[q] = S.red[q];
@@ -496,22 +742,16 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
     double nn2 = sw - dsum;
     if (!(nn2 >= 0.5 * sw)) {
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
-      for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
-        double wv = static_cast<double>(w[q]);
-#pragma unroll 8
-        for (int i = 0; i <= j; ++i) wv -= S.coef[i] * static_cast<double>(V[static_cast<long long>(i) * n + q]);
-        w[q] = static_cast<T>(wv);
-      }
-      block_dots<T>(V, n, w, rw, j + 1, true, part_row);
+      if (wide) sweep_combine<TV, true, 2>(rw, V, n, S.coef, j + 1, w, w);
+      else sweep_combine<TV, true, 1>(rw, V, n, S.coef, j + 1, w, w);
+      block_dots<TV>(V, n, w, rw, j + 1, true, part_row, S.dpart);
       if (!grid_sync(a.bar, gen, a.spin_limit)) {
         st.timeout = 1;
         return st;
       }
       grid_reduce_redundant(a.part, ld, j + 2, S.red, S.scratch);
       sw = S.red[j + 1];
-      double dd = 0.0;
-      for (int q = 0; q <= j; ++q) dd += S.red[q] * S.red[q];
-      nn2 = sw - dd;
+      nn2 = sw - sum_squares(S.red, j + 1);
       for (int q = threadIdx.x; q <= j; q += NT) {
         S.hcol[q] += S.red[q];
         S.coef[q] = S.red[q];
@@ -525,13 +765,27 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
     }
     // ---- Givens rotation of the new column (identical in every block) ----
     if (threadIdx.x == 0) {
-      S.hcol[j + 1] = nn;
-      for (int i = 0; i < j; ++i) {
-        const double h0 = S.hcol[i], h1 = S.hcol[i + 1];
-        S.hcol[i] = S.cs[i] * h0 + S.sn[i] * h1;
-        S.hcol[i + 1] = -S.sn[i] * h0 + S.cs[i] * h1;
+      // the running entry stays in a register; the rotations and the column
+      // are read 8 at a time ahead of the dependent chain
+      double hr = S.hcol[0];
+      for (int i0 = 0; i0 < j; i0 += 8) {
+        double cc[8], ss[8], hh[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int i = i0 + k < j ? i0 + k : j - 1;
+          cc[k] = S.cs[i];
+          ss[k] = S.sn[i];
+          hh[k] = S.hcol[i + 1];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          if (i0 + k < j) {
+            S.hcol[i0 + k] = cc[k] * hr + ss[k] * hh[k];
+            hr = -ss[k] * hr + cc[k] * hh[k];
+          }
+        }
       }
-      const double h0 = S.hcol[j], h1 = S.hcol[j + 1];
+      const double h0 = hr, h1 = nn;
       const double rho = hypot(h0, h1);
       S.cs[j] = rho == 0.0 ? 1.0 : h0 / rho;
       S.sn[j] = rho == 0.0 ? 0.0 : h1 / rho;
@@ -551,46 +805,20 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
     }
     broke = !(nn > btol);
     // ---- sweep C: w <- w - V coef; v_{j+1} = w / nn; r_j recurrence ----
-    T* vn = V + static_cast<long long>(j + 1) * n;
+    TV* vn = V + static_cast<long long>(j + 1) * n;
     const double inv_nn = broke ? 0.0 : 1.0 / nn;
     const double cr1 = s * s, cr2 = -s * c * gam;
-    double rmx = 0.0;
-    for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
-      double wv = static_cast<double>(w[q]);
-#pragma unroll 8
-      for (int i = 0; i <= j; ++i) wv -= S.coef[i] * static_cast<double>(V[static_cast<long long>(i) * n + q]);
-      const T vq = static_cast<T>(wv * inv_nn);
-      vn[q] = vq;
-      if (rres) {
-        const double rq = cr1 * rres[q] + cr2 * static_cast<double>(vq);
-        rres[q] = rq;
-        rmx = nanmax(rmx, fabs(rq));
-      }
-    }
+    const double rmx = wide ? sweep_next<TV, 2>(rw, V, n, S.coef, j + 1, w, vn, inv_nn, cr1, cr2, rres)
+                            : sweep_next<TV, 1>(rw, V, n, S.coef, j + 1, w, vn, inv_nn, cr1, cr2, rres);
     st.it = j + 1;
-    if (reference_rule) {
-      block_max_partial(rmx, part_row, XSLOT, S.scratch);
-    } else {
-      const double est = fabs(S.g[j + 1]);
-      st.best_it = j + 1;
-      st.best_linf = est;
-      if (est <= rtol * beta) {
-        st.converged = 1;
-        break;
-      }
-      if (broke) {
-        st.breakdown = 1;
-        break;
-      }
-      if (j + 1 >= kmax) break;
-    }
+    block_max_partial(rmx, part_row, XSLOT, S.scratch);
   }
   // ---- x = x0 + V_k y_k for the returned iterate k ----
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
     st.timeout = 1;
     return st;
   }
-  const int k = st.best_it;
+  int k = st.best_it;
   double* y = S.red;
   back_substitute(a.R, a.m + 1, S.g, k, y);
   // For k below the last rotated column, g[0..k) and R's leading k x k block
@@ -598,29 +826,22 @@ __device__ SolveState krylov(const GmresArgs& a, const T* __restrict__ bvec, con
   bool ynf = false;
   for (int q = 0; q < k; ++q) ynf |= !isfinite(y[q]);
   if (ynf) st.nonfinite = 1;
-  for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
-    double xv = static_cast<double>(x0vec[q]);
-    if (!ynf) {
-#pragma unroll 8
-      for (int i = 0; i < k; ++i) xv += y[i] * static_cast<double>(V[static_cast<long long>(i) * n + q]);
-    }
-    xvec[q] = static_cast<T>(xv);
-  }
+  if (ynf) k = 0;  // x = x0
+  if (wide) sweep_combine<TV, false, 2>(rw, V, n, y, k, x0vec, xvec);
+  else sweep_combine<TV, false, 1>(rw, V, n, y, k, x0vec, xvec);
   return st;
 }
 
 __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
 {
   extern __shared__ double sh[];
-  unsigned int gen = 0;
-  gen = ld_volatile(&a.bar->gen);  // reset to 0 by the host before the launch
-  const Rows rw = own_rows(a.n);
+  unsigned int gen = 0;  // barriers passed; the counter is zeroed by the host before the launch
   EcgGmresResult out;
   std::memset(&out, 0, sizeof(out));
   const int limit = a.max_iter < a.n ? a.max_iter : static_cast<int>(a.n);
   if (!a.mixed) {
-    const SolveState st = krylov<double>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, true,
-                                         gen, sh);
+    const SolveState st =
+        krylov<double>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, sh);
     out.iterations = st.best_it;
     out.converged = st.converged;
     out.breakdown = st.breakdown;
@@ -629,79 +850,38 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
     out.residual_linf = st.best_linf;
     out.inner_iterations = st.it;
   } else {
-    // FP64 iterative refinement around FP32 GMRES.
-    // x <- x0; repeat: r = b - A x (FP64); stop on the reference rule;
-    // solve A d = r in FP32 to inner_rtol; x <- x + d.
-    for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) a.x[q] = a.x0[q];
-    int total_inner = 0, sweeps = 0;
-    double bn = 1.0;
-    double linf = __builtin_huge_val();
-    int conv = 0, nf = 0, to = 0;
-    const Smem S = carve(sh, a.m);
-    double* tmp = S.scratch;
-    double* part_row = a.part + static_cast<long long>(blockIdx.x) * a.ld;
+    // Cycles of the FP32-basis solve; each opens with the true FP64 residual
+    // of the current iterate (x0, then x) and the reference's stopping rule.
+    int total = 0, cycles = 0;
+    const double* xin = a.x0;
+    SolveState st;
+    std::memset(&st, 0, sizeof(st));
+    const int per_cycle = a.inner_max > 0 ? a.inner_max : limit;
     for (;;) {
-      if (!grid_sync(a.bar, gen, a.spin_limit)) {
-        to = 1;
+      const int left = limit - total;
+      const bool last = cycles + 1 >= a.max_refine;
+      const int kin = per_cycle < left ? per_cycle : left;
+      st = krylov<float>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol, gen,
+                         sh);
+      ++cycles;
+      out.iterations = total + st.best_it;
+      total += st.it;
+      if (st.timeout || st.nonfinite || st.breakdown) break;
+      if (st.converged && st.it == 0) break;  // the true residual meets the rule
+      if (total >= limit || last) break;
+      xin = a.x;
+      if (!grid_sync(a.bar, gen, a.spin_limit)) {  // x complete before the next residual
+        st.timeout = 1;
         break;
       }
-      double bmax = 0.0, rmax = 0.0;
-      for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
-        const int i = static_cast<int>(q % a.op.nx), j = static_cast<int>(q / a.op.nx);
-        const double rq = a.b[q] - apply_row<double>(a.op, a.x, i, j, q);
-        bmax = nanmax(bmax, fabs(a.b[q]));
-        rmax = nanmax(rmax, fabs(rq));
-        a.r32[q] = static_cast<float>(rq);
-        a.r[q] = rq;
-      }
-      block_max_partial(bmax, part_row, 0, tmp);
-      block_max_partial(rmax, part_row, 1, tmp);
-      if (!grid_sync(a.bar, gen, a.spin_limit)) {
-        to = 1;
-        break;
-      }
-      const double braw = grid_max_redundant(a.part, a.ld, 0, tmp);
-      linf = grid_max_redundant(a.part, a.ld, 1, tmp);
-      bn = braw > 1.0 ? braw : 1.0;
-      if (!isfinite(linf) || !isfinite(braw)) {
-        nf = 1;
-        break;
-      }
-      if (linf <= a.tol || linf / bn <= a.tol) {
-        conv = 1;
-        break;
-      }
-      if (sweeps >= a.max_refine || total_inner >= limit) break;
-      // inner solve from d0 = 0 (w32 holds zeros for x0)
-      for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) a.w32[q] = 0.0f;
-      float* d32 = a.w32 + a.n;  // correction
-      for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) d32[q] = 0.0f;
-      if (!grid_sync(a.bar, gen, a.spin_limit)) {
-        to = 1;
-        break;
-      }
-      const int kin = a.inner_max < limit - total_inner ? a.inner_max : limit - total_inner;
-      const SolveState st = krylov<float>(a, a.r32, a.w32, d32, a.V32, a.w32 + 2 * a.n, nullptr, kin, 0.0,
-                                          a.inner_rtol, false, gen, sh);
-      total_inner += st.it;
-      ++sweeps;
-      if (st.timeout) {
-        to = 1;
-        break;
-      }
-      if (st.nonfinite) {
-        nf = 1;
-        break;
-      }
-      for (long long q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) a.x[q] += static_cast<double>(d32[q]);
     }
-    out.iterations = total_inner;
-    out.inner_iterations = total_inner;
-    out.refinements = sweeps;
-    out.converged = conv;
-    out.nonfinite = nf;
-    out.timeout = to;
-    out.residual_linf = linf;
+    out.converged = st.converged;
+    out.breakdown = st.breakdown;
+    out.nonfinite = st.nonfinite;
+    out.timeout = st.timeout;
+    out.residual_linf = st.best_linf;
+    out.inner_iterations = total;
+    out.refinements = cycles;
   }
   out.relative_residual_linf = 0.0;
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.res = out;
@@ -714,10 +894,11 @@ __global__ void __launch_bounds__(NT) residual_kernel(EcgPressureOp op, long lon
 {
   __shared__ double sh[NW];
   double rmax = 0.0, bmax = 0.0;
-  for (long long q = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; q < n;
-       q += static_cast<long long>(gridDim.x) * NT) {
-    const int i = static_cast<int>(q % op.nx), j = static_cast<int>(q / op.nx);
-    const double rq = apply_row<double>(op, x, i, j, q) - b[q];
+  for (int q = blockIdx.x * NT + threadIdx.x; q < n; q += gridDim.x * NT) {
+    const int qq[1] = {q};
+    double ax[1];
+    apply_rows<double, 1>(op, x, qq, ax);
+    const double rq = ax[0] - b[q];
     rmax = nanmax(rmax, fabs(rq));
     bmax = nanmax(bmax, fabs(b[q]));
   }
@@ -732,17 +913,14 @@ struct EcgGmresWork {
   int m = 0;
   int nblocks = 0;
   int device = 0;
-  bool mixed_ready = false;
+  bool mixed = false;
   double* V = nullptr;
   double* w = nullptr;
   double* r = nullptr;
   float* V32 = nullptr;
-  float* w32 = nullptr;
-  float* r32 = nullptr;
   double* part = nullptr;
   int ld = 0;
   double* R = nullptr;
-  double* yv = nullptr;
   GridBar* bar = nullptr;
   EcgGmresResult* d_res = nullptr;
   EcgGmresResult* h_res = nullptr;
@@ -752,46 +930,50 @@ struct EcgGmresWork {
 
 EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int device, bool mixed, std::string* err)
 {
+  // rows are indexed with 32-bit integers on the device
+  if (n < 1 || n > (1LL << 31) - (1LL << 24)) {
+    if (err) *err = "pressure system too large for the GMRES workspace (rows >= 2^31 - 2^24)";
+    return nullptr;
+  }
   EcgGmresWork* w = new EcgGmresWork();
   w->n = n;
   w->m = max_iter < 1 ? 1 : max_iter;
   if (w->m > n) w->m = static_cast<int>(n);
   w->device = device;
+  w->mixed = mixed;
   w->smem = smem_bytes(w->m);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_kernel, NT, w->smem);
-  if (per_sm < 1) per_sm = 1;
   // one block per SM (every SM's share of bandwidth), fewer for tiny systems
-  long long want = (n + 63) / 64;
-  long long cap = static_cast<long long>(num_sms) * (per_sm < 1 ? 1 : 1);
+  const long long want = (n + 63) / 64;
+  const long long cap = num_sms;
   w->nblocks = static_cast<int>(want < cap ? (want < 1 ? 1 : want) : cap);
   w->ld = w->m + 8;
   bool ok = true;
   auto alloc = [&](void** p, size_t bytes) {
     if (ok && cudaMalloc(p, bytes) != cudaSuccess) ok = false;
   };
-  alloc(reinterpret_cast<void**>(&w->V), sizeof(double) * (w->m + 1) * n);
+  // the basis in the precision the context solves in
+  if (mixed) alloc(reinterpret_cast<void**>(&w->V32), sizeof(float) * (w->m + 1) * n);
+  else alloc(reinterpret_cast<void**>(&w->V), sizeof(double) * (w->m + 1) * n);
   alloc(reinterpret_cast<void**>(&w->w), sizeof(double) * n);
   alloc(reinterpret_cast<void**>(&w->r), sizeof(double) * n);
   const long long part_len = static_cast<long long>(w->ld) * w->nblocks;
   alloc(reinterpret_cast<void**>(&w->part),
         sizeof(double) * (part_len > 2LL * kResidualBlocks ? part_len : 2LL * kResidualBlocks));
   alloc(reinterpret_cast<void**>(&w->R), sizeof(double) * (w->m + 1) * (w->m + 1));
-  alloc(reinterpret_cast<void**>(&w->yv), sizeof(double) * (w->m + 1));
   alloc(reinterpret_cast<void**>(&w->bar), sizeof(GridBar));
   alloc(reinterpret_cast<void**>(&w->d_res), sizeof(EcgGmresResult));
-  if (mixed) {
-    alloc(reinterpret_cast<void**>(&w->V32), sizeof(float) * (w->m + 1) * n);
-    alloc(reinterpret_cast<void**>(&w->w32), sizeof(float) * 3 * n);
-    alloc(reinterpret_cast<void**>(&w->r32), sizeof(float) * n);
-    w->mixed_ready = true;
-  }
   if (ok && cudaMallocHost(&w->h_res, sizeof(EcgGmresResult)) != cudaSuccess) ok = false;
   if (ok && cudaMallocHost(&w->h_part, sizeof(double) * 2 * kResidualBlocks) != cudaSuccess) ok = false;
   if (ok && cudaMemset(w->bar, 0, sizeof(GridBar)) != cudaSuccess) ok = false;
   if (ok && cudaFuncSetAttribute(gmres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(w->smem)) !=
                 cudaSuccess)
     ok = false;
+  int per_sm = 0;
+  if (ok && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_kernel, NT, w->smem) != cudaSuccess || per_sm < 1)) {
+    if (err) *err = "gmres kernel does not fit on one SM with its shared memory";
+    gmres_work_destroy(w);
+    return nullptr;
+  }
   if (!ok) {
     if (err) *err = "gmres workspace allocation failed";
     gmres_work_destroy(w);
@@ -807,11 +989,8 @@ void gmres_work_destroy(EcgGmresWork* w)
   cudaFree(w->w);
   cudaFree(w->r);
   cudaFree(w->V32);
-  cudaFree(w->w32);
-  cudaFree(w->r32);
   cudaFree(w->part);
   cudaFree(w->R);
-  cudaFree(w->yv);
   cudaFree(w->bar);
   cudaFree(w->d_res);
   cudaFreeHost(w->h_res);
@@ -823,7 +1002,7 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
                         int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
                         EcgGmresResult* out, cudaStream_t s)
 {
-  if (mixed && !w->mixed_ready) return cudaErrorInvalidValue;
+  if (mixed != w->mixed) return cudaErrorInvalidValue;  // the basis is allocated for one precision
   GmresArgs a;
   std::memset(&a, 0, sizeof(a));
   a.op = op;
@@ -835,11 +1014,8 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.w = w->w;
   a.r = w->r;
   a.V32 = w->V32;
-  a.w32 = w->w32;
-  a.r32 = w->r32;
   a.part = w->part;
   a.R = w->R;
-  a.yv = w->yv;
   a.bar = w->bar;
   a.res = w->d_res;
   a.ld = w->ld;
@@ -847,7 +1023,7 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.max_iter = max_iter < w->m ? max_iter : w->m;
   a.tol = tol;
   a.mixed = mixed ? 1 : 0;
-  a.inner_max = inner_max_iter < a.max_iter ? inner_max_iter : a.max_iter;
+  a.inner_max = inner_max_iter < a.max_iter ? inner_max_iter : a.max_iter;  // <= 0: no per-cycle limit
   a.inner_rtol = inner_rtol;
   a.max_refine = max_refine;
   a.spin_limit = 1LL << 25;  // ~2 s of polling before a barrier gives up

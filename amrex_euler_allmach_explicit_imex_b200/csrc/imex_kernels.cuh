@@ -476,7 +476,37 @@ __global__ void __launch_bounds__(NT) imex_rhs_kernel(const EcgImexMap m, const 
     nonfinite += rnf;
     if (isfinite(b)) bmax = umax64(bmax, okey(fabs(b)));
     else bmax = okey(kInf);
-    if (matrix_diag) {
+    const bool deep = (m.px ? m.nx >= 5 : (i >= 2 && i <= m.nx - 3)) && (m.py ? m.ny >= 5 : (j >= 2 && j <= m.ny - 3));
+    if (matrix_diag && deep) {
+      // No two of this row's columns coincide, and column r appears once in
+      // each neighbour row (the reflection and the fixed bubble columns only
+      // touch rows within two cells of a wall), so the stored entries are the
+      // raw terms and the transposed entry of each is the neighbour's raw
+      // term: the same values row_terms and its search give.
+      const double d = (1.0 / gm1 + xc * (he + hw)) + yc * (hn + hs);
+      const int ie2 = pmap(i + 2, m.nx, m.px), ie1 = pmap(i + 1, m.nx, m.px);
+      const int iw1 = pmap(i - 1, m.nx, m.px), iw2 = pmap(i - 2, m.nx, m.px);
+      const int jn2 = pmap(j + 2, m.ny, m.py), jn1 = pmap(j + 1, m.ny, m.py);
+      const int js1 = pmap(j - 1, m.ny, m.py), js2 = pmap(j - 2, m.ny, m.py);
+      const long long hr = static_cast<long long>(j) * (m.nx + 1);
+      auto HX = [&](int c) { return hx[hr + c]; };
+      auto HY = [&](int rj) { return hy[static_cast<long long>(rj) * m.nx + i]; };
+      const double a[8] = {-xc * he, -xc * (he - hw), xc * (he - hw), -xc * hw,
+                           -yc * hn, -yc * (hn - hs), yc * (hn - hs), -yc * hs};
+      const double tr[8] = {-xc * HX(ie2), xc * (HX(ie1 + 1) - HX(ie1)), -xc * (HX(iw1 + 1) - HX(iw1)), -xc * HX(iw2 + 1),
+                            -yc * HY(jn2), yc * (HY(jn1 + 1) - HY(jn1)), -yc * (HY(js1 + 1) - HY(js1)), -yc * HY(js2 + 1)};
+      unsigned long long cnt = d != 0.0 ? 1 : 0;
+      amax = umax64(amax, okey(fabs(d)));
+      sym = umax64(sym, okey(fabs(d - d)));
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        cnt += a[q] != 0.0 ? 1 : 0;
+        amax = umax64(amax, okey(fabs(a[q])));
+        sym = umax64(sym, okey(fabs(a[q] - tr[q])));
+      }
+      nnz += static_cast<long long>(cnt);
+      width = umax64(width, cnt);
+    } else if (matrix_diag) {
       RowTerms t;
       row_terms(m, hx, hy, xc, yc, i, j, t);
       nnz += t.n;

@@ -142,9 +142,9 @@ typedef struct ecg_gpu_options {
   int32_t device;           /* CUDA device ordinal */
   int32_t arith;            /* ecg_arith */
   int32_t imex_precision;   /* ecg_imex_precision */
-  int32_t mixed_inner_max_iter;  /* FP32 inner iterations per refinement sweep */
-  double mixed_inner_rtol;       /* FP32 inner relative residual target */
-  int32_t mixed_max_refinements; /* outer FP64 refinement sweeps */
+  int32_t mixed_inner_max_iter;  /* mixed: iterations per FP32-basis cycle (0: no limit) */
+  double mixed_inner_rtol;       /* mixed: restart once the recurrence residual fell by this factor (0: never) */
+  int32_t mixed_max_refinements; /* mixed: cycles, each opened with the true FP64 residual */
   int32_t tile_x;           /* column-strip kernel: rows each warp marches (0: sized so the grid fills one wave) */
   int32_t tile_y;           /* explicit kernel: 0 default (column strips, x- and y-faces
                                evaluated together), 2 column strips with faces one at a
@@ -215,8 +215,8 @@ typedef struct ecg_imex_diag {
   int32_t face_enthalpy_denominator_guard_count;
   int32_t face_enthalpy_nonfinite_count;
   int32_t energy_flux_nonfinite_count;
-  int32_t gmres_inner_iterations;     /* mixed precision: FP32 iterations (not in the reference) */
-  int32_t gmres_refinements;          /* mixed precision: FP64 refinement sweeps (not in the reference) */
+  int32_t gmres_inner_iterations;     /* mixed precision: iterations over the FP32 basis, all cycles (not in the reference) */
+  int32_t gmres_refinements;          /* mixed precision: cycles, each opened with the true FP64 residual (not in the reference) */
   double solver_initial_residual;
   double solver_initial_rhs_norm;
   double solver_residual;
