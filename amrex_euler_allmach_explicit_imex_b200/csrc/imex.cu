@@ -235,24 +235,34 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
   op.hy = im->hy;
   const double tol = c->cfg.imex_solver_tol;
 
+  // Matrix diagnostics (imex_source_map_step.hpp:466-489) of the pressure
+  // system of the current Picard pass: reported for the pass that ends the
+  // step, so they are computed there, from that pass's face enthalpies.
+  auto matrix_report = [&]() -> bool {
+    if (!reset_stats(c)) return false;
+    if (!ecgi::cuda_ok(c, ops->matrix(m, im->hx, im->hy, dt, idx, idy, im->d_st, s), "matrix diagnostics")) return false;
+    if (!fetch_stats(c)) return false;
+    d.pressure_matrix_nonzeros = static_cast<int>(st.nnz);
+    d.pressure_matrix_max_row_width = static_cast<int>(st.max_row_width);
+    d.kinetic_jacobian_abs_max = kd(st.abs_max_key);
+    d.pressure_matrix_symmetry_linf = kd(st.sym_key);
+    return true;
+  };
+
   for (int pic = 0; pic < c->cfg.imex_picard_iterations; ++pic) {
     // pressure system (source_map_build_pressure_system, imex_source_map_step.hpp:8-38,464-497)
     if (!reset_stats(c)) return ECG_ERR_CUDA;
     if (!ecgi::cuda_ok(c, ops->faces(m, im->S, im->p, im->K, im->hx, im->hy, nullptr, nullptr, 0, s), "faces"))
       return ECG_ERR_CUDA;
-    if (!ecgi::cuda_ok(c, ops->rhs(m, im->S, im->K, im->hx, im->hy, dt, idx, idy, 1, im->rhs, im->d_st, s), "rhs"))
+    if (!ecgi::cuda_ok(c, ops->rhs(m, im->S, im->K, im->hx, im->hy, dt, idx, idy, im->rhs, im->d_st, s), "rhs"))
       return ECG_ERR_CUDA;
     if (!fetch_stats(c)) return ECG_ERR_CUDA;
     d.pressure_matrix_rows = static_cast<int>(n);
-    d.pressure_matrix_nonzeros = static_cast<int>(st.nnz);
-    d.pressure_matrix_max_row_width = static_cast<int>(st.max_row_width);
-    d.kinetic_jacobian_abs_max = kd(st.abs_max_key);
-    d.pressure_matrix_symmetry_linf = kd(st.sym_key);
     if (st.row_nonfinite > 0 || !std::isfinite(kd(st.rhs_linf_key))) {
       d.solver_status = ECG_SOLVER_SOURCE_MAP_PRESSURE_ROW_NONFINITE;
       d.kinetic_lag_nonfinite_count = static_cast<int>(st.row_nonfinite);
       d.nonfinite_count = static_cast<int>(st.row_nonfinite);
-      return ECG_OK;
+      return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
     }
     double r0 = 0.0, bn = 1.0;
     int nf = 0;
@@ -288,12 +298,12 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
       if (!std::isfinite(lr) || nf) {
         d.solver_status = ECG_SOLVER_LINEAR_RESIDUAL_NONFINITE;
         d.nonfinite_count = 1;
-        return ECG_OK;
+        return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
       }
     }
     if (!abs_ok && !rel_ok) {
       d.solver_status = g.breakdown ? ECG_SOLVER_GMRES_BREAKDOWN_NOT_CONVERGED : ECG_SOLVER_LINEAR_SOLVE_NOT_CONVERGED;
-      return ECG_OK;
+      return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
     }
     // p <- x, eq54 momentum refresh (imex_source_map_step.hpp:536-564)
     if (!reset_stats(c)) return ECG_ERR_CUDA;
@@ -305,7 +315,7 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     if (st.k_nonfinite > 0) {
       d.solver_status = ECG_SOLVER_SOURCE_MAP_LAGGED_MOMENTUM_NONFINITE;
       d.nonfinite_count = d.kinetic_lag_nonfinite_count;
-      return ECG_OK;
+      return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
     }
     ++d.kinetic_lag_update_count;
     d.pressure_picard_delta_linf = kd(st.delta_linf_key);
@@ -314,6 +324,7 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     ++d.picard_pressure_solves_used;
   }
   d.solver_status = d.linear_solver_status_last;
+  if (c->cfg.imex_picard_iterations > 0 && !matrix_report()) return ECG_ERR_CUDA;
 
   // conservative closeout (evaluate_source_map_final, imex_source_map_step.hpp:75-258)
   if (!reset_stats(c)) return ECG_ERR_CUDA;

@@ -53,7 +53,9 @@ struct EcgImexOps {
   cudaError_t (*faces)(const EcgImexMap& m, const double* S, const double* p, const double* K, double* fx, double* fy,
                        unsigned char* fxf, unsigned char* fyf, int mode, cudaStream_t s);
   cudaError_t (*rhs)(const EcgImexMap& m, const double* S, const double* K, const double* hx, const double* hy,
-                     double dt, double idx, double idy, int matrix_diag, double* rhs, EcgImexStats* st, cudaStream_t s);
+                     double dt, double idx, double idy, double* rhs, EcgImexStats* st, cudaStream_t s);
+  cudaError_t (*matrix)(const EcgImexMap& m, const double* hx, const double* hy, double dt, double idx, double idy,
+                        EcgImexStats* st, cudaStream_t s);
   cudaError_t (*p_update)(long long n, double* p, const double* x, EcgImexStats* st, cudaStream_t s);
   cudaError_t (*momentum)(const EcgImexMap& m, const double* S, const double* p, double dt, double idx, double idy,
                           double* K, EcgImexStats* st, cudaStream_t s);

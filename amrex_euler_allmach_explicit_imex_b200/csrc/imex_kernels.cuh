@@ -401,25 +401,22 @@ __device__ __forceinline__ void row_terms(const EcgImexMap& m, const double* __r
 }
 
 // Right-hand side of source_map_pressure_row_data
-// (imex_source_map_helpers.hpp:488-570) with its nonfinite count, plus the
-// matrix diagnostics of the Picard loop (imex_source_map_step.hpp:466-489):
-// stored entries, widest row, largest |a_ij|, max |A - A^T|.
+// (imex_source_map_helpers.hpp:488-570) with its nonfinite count.
 template <int NT>
 __global__ void __launch_bounds__(NT) imex_rhs_kernel(const EcgImexMap m, const double* __restrict__ S,
                                                       const double* __restrict__ K, const double* __restrict__ hx,
                                                       const double* __restrict__ hy, const double dt, const double idx,
-                                                      const double idy, const int matrix_diag, double* __restrict__ rhs,
+                                                      const double idy, double* __restrict__ rhs,
                                                       EcgImexStats* __restrict__ st)
 {
   __shared__ Shared sh;
-  const long long n = static_cast<long long>(m.nx) * m.ny;
+  const int n = m.nx * m.ny;  // rows fit 32-bit indices (the GMRES workspace rejects larger systems)
   const double gm1 = m.gamma - 1.0;
   const double xc = 0.25 * dt * dt * idx * idx, yc = 0.25 * dt * dt * idy * idy;
-  long long nonfinite = 0, nnz = 0;
-  unsigned long long width = 0, amax = okey(0.0), sym = okey(0.0), bmax = okey(0.0);
-  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
-       r += static_cast<long long>(gridDim.x) * NT) {
-    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+  long long nonfinite = 0;
+  unsigned long long bmax = okey(0.0);
+  for (int r = blockIdx.x * NT + threadIdx.x; r < n; r += gridDim.x * NT) {
+    const int j = r / m.nx, i = r - j * m.nx;
     const double he = hx[static_cast<long long>(j) * (m.nx + 1) + i + 1];
     const double hw = hx[static_cast<long long>(j) * (m.nx + 1) + i];
     const double hn = hy[static_cast<long long>(j + 1) * m.nx + i];
@@ -476,60 +473,186 @@ __global__ void __launch_bounds__(NT) imex_rhs_kernel(const EcgImexMap m, const 
     nonfinite += rnf;
     if (isfinite(b)) bmax = umax64(bmax, okey(fabs(b)));
     else bmax = okey(kInf);
-    const bool deep = (m.px ? m.nx >= 5 : (i >= 2 && i <= m.nx - 3)) && (m.py ? m.ny >= 5 : (j >= 2 && j <= m.ny - 3));
-    if (matrix_diag && deep) {
-      // No two of this row's columns coincide, and column r appears once in
-      // each neighbour row (the reflection and the fixed bubble columns only
-      // touch rows within two cells of a wall), so the stored entries are the
-      // raw terms and the transposed entry of each is the neighbour's raw
-      // term: the same values row_terms and its search give.
-      const double d = (1.0 / gm1 + xc * (he + hw)) + yc * (hn + hs);
-      const int ie2 = pmap(i + 2, m.nx, m.px), ie1 = pmap(i + 1, m.nx, m.px);
-      const int iw1 = pmap(i - 1, m.nx, m.px), iw2 = pmap(i - 2, m.nx, m.px);
-      const int jn2 = pmap(j + 2, m.ny, m.py), jn1 = pmap(j + 1, m.ny, m.py);
-      const int js1 = pmap(j - 1, m.ny, m.py), js2 = pmap(j - 2, m.ny, m.py);
-      const long long hr = static_cast<long long>(j) * (m.nx + 1);
-      auto HX = [&](int c) { return hx[hr + c]; };
-      auto HY = [&](int rj) { return hy[static_cast<long long>(rj) * m.nx + i]; };
-      const double a[8] = {-xc * he, -xc * (he - hw), xc * (he - hw), -xc * hw,
-                           -yc * hn, -yc * (hn - hs), yc * (hn - hs), -yc * hs};
-      const double tr[8] = {-xc * HX(ie2), xc * (HX(ie1 + 1) - HX(ie1)), -xc * (HX(iw1 + 1) - HX(iw1)), -xc * HX(iw2 + 1),
-                            -yc * HY(jn2), yc * (HY(jn1 + 1) - HY(jn1)), -yc * (HY(js1 + 1) - HY(js1)), -yc * HY(js2 + 1)};
-      unsigned long long cnt = d != 0.0 ? 1 : 0;
-      amax = umax64(amax, okey(fabs(d)));
-      sym = umax64(sym, okey(fabs(d - d)));
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        cnt += a[q] != 0.0 ? 1 : 0;
-        amax = umax64(amax, okey(fabs(a[q])));
-        sym = umax64(sym, okey(fabs(a[q] - tr[q])));
-      }
-      nnz += static_cast<long long>(cnt);
-      width = umax64(width, cnt);
-    } else if (matrix_diag) {
-      RowTerms t;
-      row_terms(m, hx, hy, xc, yc, i, j, t);
-      nnz += t.n;
-      width = umax64(width, static_cast<unsigned long long>(t.n));
-      for (int q = 0; q < t.n; ++q) {
-        amax = umax64(amax, okey(fabs(t.val[q])));
-        // matching entry of the transpose: row t.col[q], column r
-        const int ci2 = t.col[q] % m.nx, cj2 = t.col[q] / m.nx;
-        RowTerms u2;
-        row_terms(m, hx, hy, xc, yc, ci2, cj2, u2);
-        double tv = 0.0;
-        for (int s2 = 0; s2 < u2.n; ++s2)
-          if (u2.col[s2] == static_cast<int>(r)) tv = u2.val[s2];
-        sym = umax64(sym, okey(fabs(t.val[q] - tv)));
-      }
-    }
   }
   ECG_RED_ADD_I(st->row_nonfinite, nonfinite);
+  ECG_RED_MAX(st->rhs_linf_key, bmax);
+}
+
+// ---- matrix diagnostics of the Picard loop (imex_source_map_step.hpp:466-489) ----------------
+// Stored entries, widest row, largest |a_ij| and max |A - A^T| of the pressure
+// matrix as setFromTriplets stores it (row_terms).  They are reported for the
+// Picard pass that ends the step, so the step computes them once, there.
+
+__device__ __forceinline__ bool interior_row(const EcgImexMap& m, int i, int j)
+{
+  return (m.px ? m.nx >= 5 : (i >= 2 && i <= m.nx - 3)) && (m.py ? m.ny >= 5 : (j >= 2 && j <= m.ny - 3));
+}
+
+__device__ __forceinline__ double nanmax_d(double a, double v) { return (a < v || v != v) ? v : a; }
+
+// Rows away from the walls: no two columns of the row coincide and column r
+// appears once in each neighbour row (the reflection and the fixed bubble
+// columns only touch rows within two cells of a wall), so the stored entries
+// are the raw terms and the transposed entry of each is the neighbour's raw
+// term.  Maxima are kept in FP64 (NaN wins) and keyed once per thread.
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_matrix_interior_kernel(const EcgImexMap m, const double* __restrict__ hx,
+                                                                  const double* __restrict__ hy, const double xc,
+                                                                  const double yc, EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const int nx = m.nx, n = m.nx * m.ny;
+  const double gi = 1.0 / (m.gamma - 1.0);
+  long long nnz = 0;
+  unsigned long long width = 0;
+  double amax = 0.0, sym = 0.0;
+  for (int r = blockIdx.x * NT + threadIdx.x; r < n; r += gridDim.x * NT) {
+    const int j = r / nx, i = r - j * nx;
+    if (!interior_row(m, i, j)) continue;
+    const int hr = j * (nx + 1);
+    const double he = hx[hr + i + 1], hw = hx[hr + i];
+    const double hn = hy[(j + 1) * nx + i], hs = hy[j * nx + i];
+    const int ie2 = pmap(i + 2, nx, m.px), ie1 = pmap(i + 1, nx, m.px);
+    const int iw1 = pmap(i - 1, nx, m.px), iw2 = pmap(i - 2, nx, m.px);
+    const int jn2 = pmap(j + 2, m.ny, m.py), jn1 = pmap(j + 1, m.ny, m.py);
+    const int js1 = pmap(j - 1, m.ny, m.py), js2 = pmap(j - 2, m.ny, m.py);
+    const double d = (gi + xc * (he + hw)) + yc * (hn + hs);
+    const double a[8] = {-xc * he, -xc * (he - hw), xc * (he - hw), -xc * hw,
+                         -yc * hn, -yc * (hn - hs), yc * (hn - hs), -yc * hs};
+    const double tr[8] = {-xc * hx[hr + ie2],
+                          xc * (hx[hr + ie1 + 1] - hx[hr + ie1]),
+                          -xc * (hx[hr + iw1 + 1] - hx[hr + iw1]),
+                          -xc * hx[hr + iw2 + 1],
+                          -yc * hy[jn2 * nx + i],
+                          yc * (hy[(jn1 + 1) * nx + i] - hy[jn1 * nx + i]),
+                          -yc * (hy[(js1 + 1) * nx + i] - hy[js1 * nx + i]),
+                          -yc * hy[(js2 + 1) * nx + i]};
+    int cnt = d != 0.0 ? 1 : 0;
+    amax = nanmax_d(amax, fabs(d));
+    sym = nanmax_d(sym, fabs(d - d));
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      cnt += a[q] != 0.0 ? 1 : 0;
+      amax = nanmax_d(amax, fabs(a[q]));
+      sym = nanmax_d(sym, fabs(a[q] - tr[q]));
+    }
+    nnz += cnt;
+    width = umax64(width, static_cast<unsigned long long>(cnt));
+  }
   ECG_RED_ADD_I(st->nnz, nnz);
   ECG_RED_MAX(st->max_row_width, width);
-  ECG_RED_MAX(st->abs_max_key, amax);
-  ECG_RED_MAX(st->sym_key, sym);
-  ECG_RED_MAX(st->rhs_linf_key, bmax);
+  ECG_RED_MAX(st->abs_max_key, okey(amax));
+  ECG_RED_MAX(st->sym_key, okey(sym));
+}
+
+// The eleven lhs terms of row (i, j) in insertion order (row_terms before the
+// merge): column and value, and whether the term is left out (a fixed bubble
+// column, or a zero value).
+struct RowRaw {
+  int col[11];
+  double val[11];
+  bool out[11];
+};
+__device__ __forceinline__ void row_raw(const EcgImexMap& m, const double* __restrict__ hx, const double* __restrict__ hy,
+                                        double xc, double yc, int i, int j, RowRaw& t)
+{
+  const double he = hx[j * (m.nx + 1) + i + 1], hw = hx[j * (m.nx + 1) + i];
+  const double hn = hy[(j + 1) * m.nx + i], hs = hy[j * m.nx + i];
+  const int ci[11] = {i, i + 2, i + 1, i, i - 1, i - 2, i, i, i, i, i};
+  const int cj[11] = {j, j, j, j, j, j, j + 2, j + 1, j, j - 1, j - 2};
+  const double cv[11] = {1.0 / (m.gamma - 1.0), -xc * he, -xc * (he - hw), xc * (he + hw), xc * (he - hw),
+                         -xc * hw, -yc * hn, -yc * (hn - hs), yc * (hn + hs), yc * (hn - hs), -yc * hs};
+#pragma unroll
+  for (int q = 0; q < 11; ++q) {
+    t.out[q] = (m.bubble && !m.px && ci[q] < 0) || cv[q] == 0.0;
+    t.col[q] = prow(m, ci[q], cj[q]);
+    t.val[q] = cv[q];
+  }
+}
+
+// Stored value of row (i, j) at column c (duplicates summed in insertion
+// order, as setFromTriplets does); false when the row stores nothing there.
+__device__ __forceinline__ bool row_entry(const EcgImexMap& m, const double* __restrict__ hx,
+                                          const double* __restrict__ hy, double xc, double yc, int i, int j, int c,
+                                          double& v)
+{
+  RowRaw t;
+  row_raw(m, hx, hy, xc, yc, i, j, t);
+  bool found = false;
+  v = 0.0;
+#pragma unroll
+  for (int q = 0; q < 11; ++q)
+    if (!t.out[q] && t.col[q] == c) {
+      v = found ? v + t.val[q] : t.val[q];
+      found = true;
+    }
+  return found;
+}
+
+// Rows within two cells of a wall (every row when a periodic axis has fewer
+// than five cells): the merged row and, for each stored entry, the stored
+// entry of the transposed row; all in registers.  Threads walk the ring of
+// such rows only: x-edge columns of every row, then the y-edge rows' other
+// columns.
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_matrix_edge_kernel(const EcgImexMap m, const double* __restrict__ hx,
+                                                              const double* __restrict__ hy, const double xc,
+                                                              const double yc, EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const int nx = m.nx, ny = m.ny;
+  const bool all = (m.px && nx < 5) || (m.py && ny < 5);
+  const int xcnt = m.px ? 0 : (nx >= 5 ? 4 : nx), ycnt = m.py ? 0 : (ny >= 5 ? 4 : ny);
+  const int inner = nx - xcnt;  // columns outside the x ring
+  const int slots = all ? nx * ny : xcnt * ny + inner * ycnt;
+  long long nnz = 0;
+  unsigned long long width = 0;
+  double amax = 0.0, sym = 0.0;
+  for (int t = blockIdx.x * NT + threadIdx.x; t < slots; t += gridDim.x * NT) {
+    int i, j;
+    if (all) {
+      j = t / nx;
+      i = t - j * nx;
+    } else if (t < xcnt * ny) {
+      j = t / xcnt;
+      const int k = t - j * xcnt;
+      i = xcnt == nx ? k : (k < 2 ? k : nx - 4 + k);
+    } else {
+      const int u = t - xcnt * ny;
+      const int kr = inner > 0 ? u / inner : 0;
+      i = (xcnt == 0 ? 0 : 2) + (u - kr * inner);
+      j = ycnt == ny ? kr : (kr < 2 ? kr : ny - 4 + kr);
+    }
+    const int r = j * nx + i;
+    RowRaw a;
+    row_raw(m, hx, hy, xc, yc, i, j, a);
+    int cnt = 0;
+#pragma unroll
+    for (int q = 0; q < 11; ++q) {
+      if (a.out[q]) continue;
+      bool first = true;
+#pragma unroll
+      for (int p = 0; p < q; ++p)
+        if (!a.out[p] && a.col[p] == a.col[q]) first = false;
+      if (!first) continue;
+      ++cnt;
+      double v = a.val[q];  // merged value: the later duplicates, in order
+#pragma unroll
+      for (int p = q + 1; p < 11; ++p)
+        if (!a.out[p] && a.col[p] == a.col[q]) v = v + a.val[p];
+      amax = nanmax_d(amax, fabs(v));
+      const int c = a.col[q];
+      double tv;
+      if (!row_entry(m, hx, hy, xc, yc, c % nx, c / nx, r, tv)) tv = 0.0;
+      sym = nanmax_d(sym, fabs(v - tv));
+    }
+    nnz += cnt;
+    width = umax64(width, static_cast<unsigned long long>(cnt));
+  }
+  ECG_RED_ADD_I(st->nnz, nnz);
+  ECG_RED_MAX(st->max_row_width, width);
+  ECG_RED_MAX(st->abs_max_key, okey(amax));
+  ECG_RED_MAX(st->sym_key, okey(sym));
 }
 
 // ---- p update and eq54 momentum -----------------------------------------------------------
@@ -805,12 +928,23 @@ inline cudaError_t imex_faces(const EcgImexMap& m, const double* S, const double
 }
 
 inline cudaError_t imex_rhs(const EcgImexMap& m, const double* S, const double* K, const double* hx, const double* hy,
-                            double dt, double idx, double idy, int matrix_diag, double* rhs, EcgImexStats* st,
-                            cudaStream_t s)
+                            double dt, double idx, double idy, double* rhs, EcgImexStats* st, cudaStream_t s)
 {
   const long long n = static_cast<long long>(m.nx) * m.ny;
-  imexk::imex_rhs_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, K, hx, hy, dt, idx, idy, matrix_diag,
-                                                                         rhs, st);
+  imexk::imex_rhs_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, K, hx, hy, dt, idx, idy, rhs, st);
+  return cudaGetLastError();
+}
+
+// nnz, widest row, largest |a_ij| and max |A - A^T| into st (zeroed by the caller)
+inline cudaError_t imex_matrix(const EcgImexMap& m, const double* hx, const double* hy, double dt, double idx,
+                               double idy, EcgImexStats* st, cudaStream_t s)
+{
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  const double xc = 0.25 * dt * dt * idx * idx, yc = 0.25 * dt * dt * idy * idy;
+  imexk::imex_matrix_interior_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, hx, hy, xc, yc, st);
+  const long long ring = 4LL * (m.nx + m.ny);
+  imexk::imex_matrix_edge_kernel<128><<<imexk::blocks_for(n < 2 * ring ? n : ring, 128), 128, 0, s>>>(m, hx, hy, xc,
+                                                                                                       yc, st);
   return cudaGetLastError();
 }
 
