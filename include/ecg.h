@@ -135,7 +135,7 @@ typedef enum ecg_arith {
 /* Precision of the IMEX pressure solve. */
 typedef enum ecg_imex_precision {
   ECG_IMEX_FP64 = 0,   /* all-FP64 GMRES */
-  ECG_IMEX_MIXED = 1   /* FP32 inner GMRES, FP64 residual + iterative refinement */
+  ECG_IMEX_MIXED = 1   /* FP32-stored Krylov basis, FP64 arithmetic, restarts from the true FP64 residual */
 } ecg_imex_precision;
 
 typedef struct ecg_gpu_options {
