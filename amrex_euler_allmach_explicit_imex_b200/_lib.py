@@ -35,6 +35,12 @@ SIGNATURES = {
     "ecg_synchronize": (C.c_int, [_CTX]),
     "ecg_initialize_state": (C.c_int, [_CTX]),
     "ecg_paper_t1s2_run": (C.c_int, [_CTX, C.POINTER(abi.PaperOptions), C.POINTER(abi.PaperResult)]),
+    "ecg_measure_fp64_peak": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
+    "ecg_write_final_csv": (C.c_int, [_CTX, C.c_char_p, C.POINTER(abi.OutputInfo)]),
+    "ecg_shock_bubble_metrics": (C.c_int, [_CTX, C.c_double, C.POINTER(abi.BubbleMetrics)]),
+    "ecg_write_bubble_snapshot": (C.c_int, [_CTX, C.c_char_p, C.c_int32, C.c_int32, C.c_double, C.c_int32]),
+    "ecg_output_wait": (C.c_int, [_CTX, C.POINTER(C.c_int32)]),
+    "ecg_write_bubble_summary_csv": (C.c_int, [_CTX, C.c_char_p, C.POINTER(abi.BubbleRun)]),
     "ecg_euler_fv_one_step": (C.c_int, [_CTX, _D, _D, C.POINTER(_I32)]),
     "ecg_compute_euler_dt": (C.c_int, [_CTX, _D, C.POINTER(_D)]),
     "ecg_compute_imex_dt": (C.c_int, [_CTX, _D, C.POINTER(_D), C.POINTER(abi.ImexTimestepDiag)]),

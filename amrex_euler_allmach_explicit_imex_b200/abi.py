@@ -217,6 +217,41 @@ class PaperResult(C.Structure):
     ]
 
 
+class OutputInfo(C.Structure):
+    _fields_ = [
+        ("step", C.c_int32),
+        ("pad", C.c_int32),
+        ("time", C.c_double),
+        ("trial_density_min", C.c_double),
+        ("trial_pressure_min", C.c_double),
+        ("trial_internal_energy_min", C.c_double),
+    ]
+
+
+class BubbleMetrics(C.Structure):
+    _fields_ = [(f, C.c_double) for f in (
+        "rho_min", "rho_max", "pressure_min", "pressure_max", "internal_energy_min", "density_bubble_centroid_x",
+        "density_bubble_centroid_y", "density_bubble_area", "density_bubble_area_threshold", "schlieren_max")] + [
+        ("nonfinite_count", C.c_int32), ("pad", C.c_int32)]
+
+
+class BubbleRun(C.Structure):
+    _fields_ = [
+        ("steps_accepted", C.c_int32),
+        ("steps_rejected", C.c_int32),
+        ("time", C.c_double),
+        ("wall_time_sec", C.c_double),
+        ("dt_min", C.c_double),
+        ("dt_max", C.c_double),
+        ("dt_mean", C.c_double),
+        ("status", C.c_char_p),
+        ("failure_category", C.c_char_p),
+        ("snapshot_status", C.c_char_p),
+        ("snapshot_dir", C.c_char_p),
+        ("snapshot_times", C.c_char_p),
+    ]
+
+
 # euler.bdltv20_paper_t1_s2 settings (ecg_paper_mode)
 PAPER_MODE = {
     "off": 0,

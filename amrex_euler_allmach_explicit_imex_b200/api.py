@@ -22,6 +22,7 @@ The MultiFab becomes a Context holding the device state; numpy arrays of
 shape (4, ny, nx) (components rho, mx, my, E) move it in and out.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -202,8 +203,61 @@ def run_bdltv20_paper_t1_s2(ctx, settings):
     driver, and returns its report (abi.PaperResult)."""
     o = paper_options(settings)
     r = abi.PaperResult()
-    check(load().ecg_paper_t1s2_run(ctx.handle, C.byref(o), C.byref(r)), "run_bdltv20_paper_t1_s2", ctx.handle)
+    check(load().ecg_paper_t1s2_run(ctx.handle, C.byref(o), C.byref(r)), "run_bdltv20_paper_t1_s2", "measure_fp64_peak", ctx.handle)
     return r
+
+
+def write_final_csv(ctx, path, step, time, trial_minima=(float("nan"),) * 3):
+    """The problem's final CSV (write_gresho_final_csv, write_toro_final_csv,
+    write_riemann_quadrant_final_csv or write_advection_blob_final_csv,
+    io/output_cases.hpp:16-216) of the context's state."""
+    info = abi.OutputInfo()
+    info.step, info.time = int(step), float(time)
+    info.trial_density_min, info.trial_pressure_min, info.trial_internal_energy_min = map(float, trial_minima)
+    check(load().ecg_write_final_csv(ctx.handle, os.fsencode(path), C.byref(info)), "write_final_csv", ctx.handle)
+
+
+def shock_bubble_metrics(ctx, time=0.0):
+    """compute_shock_density_bubble_metrics (io/output_cases.hpp:329-403)."""
+    m = abi.BubbleMetrics()
+    check(load().ecg_shock_bubble_metrics(ctx.handle, float(time), C.byref(m)), "shock_bubble_metrics", ctx.handle)
+    return m
+
+
+def write_bubble_snapshot(ctx, directory, index, step, time, asynchronous=False):
+    """write_shock_density_bubble_snapshot (io/output_cases.hpp:405-487); with
+    asynchronous=True the file is written by a host thread while stepping
+    goes on (output_wait joins)."""
+    check(load().ecg_write_bubble_snapshot(ctx.handle, os.fsencode(directory), int(index), int(step), float(time),
+                                           1 if asynchronous else 0), "write_bubble_snapshot", ctx.handle)
+
+
+def output_wait(ctx):
+    """Joins the asynchronous snapshot writers."""
+    failed = C.c_int32()
+    check(load().ecg_output_wait(ctx.handle, C.byref(failed)), "output_wait", ctx.handle)
+
+
+def write_bubble_summary_csv(ctx, path, steps_accepted, time, status="ok", failure_category="ok", steps_rejected=0,
+                             wall_time_sec=0.0, dt_min=float("nan"), dt_max=float("nan"), dt_mean=float("nan"),
+                             snapshot_status="not_requested", snapshot_dir="",
+                             snapshot_times="0,0.06,0.12,0.18,0.24,0.30"):
+    """write_shock_density_bubble_summary_csv (io/output_cases.hpp:489-588)."""
+    r = abi.BubbleRun()
+    r.steps_accepted, r.steps_rejected, r.time = int(steps_accepted), int(steps_rejected), float(time)
+    r.wall_time_sec, r.dt_min, r.dt_max, r.dt_mean = map(float, (wall_time_sec, dt_min, dt_max, dt_mean))
+    r.status, r.failure_category, r.snapshot_status = status.encode(), failure_category.encode(), snapshot_status.encode()
+    r.snapshot_dir, r.snapshot_times = snapshot_dir.encode(), snapshot_times.encode()
+    check(load().ecg_write_bubble_summary_csv(ctx.handle, os.fsencode(path), C.byref(r)), "write_bubble_summary_csv",
+          ctx.handle)
+
+
+def measure_fp64_peak(device=0):
+    """FP64 FMA throughput of `device` in TFLOP/s (ecg_measure_fp64_peak): the
+    denominator of the explicit step's FP64 roofline."""
+    v = C.c_double()
+    check(load().ecg_measure_fp64_peak(device, C.byref(v)), "measure_fp64_peak")
+    return v.value
 
 
 class Batch:

@@ -37,6 +37,8 @@ SOURCES = {
     "batched.cu": ["-fmad=true"],
     "adjoint.cu": ["-fmad=true"],
     "noalloc.cu": [],
+    "peak.cu": [],
+    "output.cu": ["-fmad=false"],
     "paper.cu": ["-fmad=false"],
 }
 

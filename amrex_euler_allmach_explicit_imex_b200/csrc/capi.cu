@@ -235,6 +235,7 @@ ecg_ctx::~ecg_ctx()
     if (g.exec) cudaGraphExecDestroy(g.exec);
   }
   imex_free(this);
+  output_destroy(out);
   cudaFree(d_state[0]);
   cudaFree(d_state[1]);
   cudaFree(d_ring);
@@ -261,6 +262,7 @@ const char* ecg_status_str(ecg_status s)
     case ECG_ERR_NO_DEVICE: return "no usable sm_100 device";
     case ECG_ERR_UNSUPPORTED: return "unsupported configuration";
     case ECG_ERR_NOT_READY: return "state not uploaded";
+    case ECG_ERR_IO: return "output file not written";
   }
   return "unknown status";
 }

@@ -10,6 +10,7 @@
 #include "ecg_internal.h"
 
 struct EcgImexState;  // imex.cu
+struct EcgOutput;     // output.cu
 
 struct ecg_ctx {
   static constexpr int kChunk = 32;  // explicit steps per captured graph
@@ -56,6 +57,7 @@ struct ecg_ctx {
   std::vector<Graph> graphs;
 
   EcgImexState* imex = nullptr;
+  EcgOutput* out = nullptr;  // output writers' buffers (output.cu)
   // adjoint workspace (adjoint.cu): primitive gradients, one stats record
   double* adj_gq = nullptr;
   EcgStepStats* adj_stats = nullptr;
@@ -85,4 +87,6 @@ bool fetch_fused(ecg_ctx* c);
 
 // imex.cu
 void imex_free(ecg_ctx* c);
+// output.cu
+void output_destroy(EcgOutput* o);
 ecg_status imex_run(ecg_ctx* c, int32_t max_step, double stop_time, ecg_run_result* out);

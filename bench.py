@@ -89,13 +89,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+def step_profile():
+    """The committed ncu summary of the step kernel: DRAM bytes per launch and
+    FP64 flops per cell (opcode counts of the same capture)."""
     p = os.path.join(ROOT, "profiles", "fv_march_hllc_bubble_2560x640.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch")
-    return None
+            return json.load(f)
+    return {}
 
 
 class ClockSampler:
@@ -374,6 +375,7 @@ def run_ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     flush_sink = torch.empty((), dtype=torch.float32, device=dev)
     cells = NX * NY
+    fp64_peak = api.measure_fp64_peak(local)  # TFLOP/s on this GPU, before the timed region
 
     def one_step(t):
         dt = api.compute_euler_dt(ctx, t)
@@ -449,14 +451,22 @@ def run_ours(args):
         if world == 1 and not args.no_cpu_baseline:
             v, kind, cores, sample = cpu_reference_step_rate(args.cpu_steps, os.cpu_count())
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
-        traffic = profile_traffic()
+        prof = step_profile()
+        traffic = prof.get("dram_bytes_per_launch")
+        fpc = prof.get("fp64_flop_per_cell")
+        fp64 = None
+        if fpc:
+            got = fpc * cells / kern_s / 1e12
+            fp64 = {"achieved": got, "peak": fp64_peak, "unit": "TFLOP/s", "frac": got / fp64_peak if fp64_peak else None,
+                    "flop_per_cell": fpc, "peak_source": "ecg_measure_fp64_peak on this GPU (independent FMA chains)",
+                    "note": "FP64 flops per cell from the ncu opcode counts of the step kernel (2 DFMA + DMUL + DADD)"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (the shock-density-bubble initial condition of the reference's initialize_state, written on the device)", "config": CONFIG,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_source": peak_kind,
+                         "traffic": traffic, "peak_source": peak_kind, "fp64": fp64,
                          "note": "algorithmic bytes = 64 B x 1,638,400 cells per launch; event time of the fused step kernel"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * cells,
                     "d2h_bytes_per_step": 32 * cells},

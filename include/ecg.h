@@ -34,7 +34,8 @@ typedef enum ecg_status {
   ECG_ERR_TIMEOUT = 3,      /* a bounded device-side wait gave up */
   ECG_ERR_NO_DEVICE = 4,    /* no usable sm_100 device */
   ECG_ERR_UNSUPPORTED = 5,  /* configuration outside the rebuilt hot path */
-  ECG_ERR_NOT_READY = 6     /* state not uploaded yet */
+  ECG_ERR_NOT_READY = 6,    /* state not uploaded yet */
+  ECG_ERR_IO = 7            /* an output file could not be written */
 } ecg_status;
 
 /* Mirrors ProblemKind (core/solver_types.hpp:2-10), same order. */
@@ -399,6 +400,63 @@ ecg_status ecg_run(ecg_ctx* ctx, int32_t max_step, double stop_time, ecg_run_res
  * context.  The configuration must satisfy the reference's checks for the
  * mode (core/config_reader.hpp:133-258), else ECG_ERR_BAD_ARG. */
 ecg_status ecg_paper_t1s2_run(ecg_ctx* ctx, const ecg_paper_options* opts, ecg_paper_result* out);
+
+/* ---- output writers (io/output_cases.hpp) -------------------------------- */
+/* The run's files in the reference's formats: columns computed on the device
+ * in the reference's arithmetic, rows printed with %.17g (its
+ * std::setprecision(17)) by all host threads. */
+typedef struct ecg_output_info {
+  int32_t step;
+  int32_t pad;
+  double time;
+  /* Gresho file only: the IMEX admissibility run minima (NaN for explicit runs,
+   * as the driver passes them, app/driver_main.hpp:350-358) */
+  double trial_density_min, trial_pressure_min, trial_internal_energy_min;
+} ecg_output_info;
+
+typedef struct ecg_bubble_metrics {  /* ShockDensityBubbleMetrics, io/output_cases.hpp:253-265 */
+  double rho_min, rho_max, pressure_min, pressure_max, internal_energy_min;
+  double density_bubble_centroid_x, density_bubble_centroid_y, density_bubble_area;
+  double density_bubble_area_threshold, schlieren_max;
+  int32_t nonfinite_count;
+  int32_t pad;
+} ecg_bubble_metrics;
+
+typedef struct ecg_bubble_run {  /* run-level fields of the bubble summary, from the driver */
+  int32_t steps_accepted, steps_rejected;
+  double time, wall_time_sec, dt_min, dt_max, dt_mean;
+  const char* status;
+  const char* failure_category;
+  const char* snapshot_status;
+  const char* snapshot_dir;
+  const char* snapshot_times;
+} ecg_bubble_run;
+
+/* write_gresho_final_csv / write_toro_final_csv / write_riemann_quadrant_final_csv
+ * / write_advection_blob_final_csv (io/output_cases.hpp:16-216), chosen by the
+ * configured problem; ECG_ERR_UNSUPPORTED for other problems. */
+ecg_status ecg_write_final_csv(ecg_ctx* ctx, const char* path, const ecg_output_info* info);
+/* compute_shock_density_bubble_metrics (io/output_cases.hpp:329-403) of the
+ * current state: one device reduction (the area and centroid sums are
+ * summed in a different order than the reference's loop). */
+ecg_status ecg_shock_bubble_metrics(ecg_ctx* ctx, double time, ecg_bubble_metrics* out);
+/* write_shock_density_bubble_snapshot (io/output_cases.hpp:405-487) of the
+ * current state into dir.  async != 0: the columns are copied on a side
+ * stream and a host thread writes the file while the caller keeps stepping
+ * (two in flight; ecg_output_wait joins them). */
+ecg_status ecg_write_bubble_snapshot(ecg_ctx* ctx, const char* dir, int32_t index, int32_t step, double time,
+                                     int32_t async);
+/* Waits for the asynchronous snapshots; *failed = files not written. */
+ecg_status ecg_output_wait(ecg_ctx* ctx, int32_t* failed);
+/* write_shock_density_bubble_summary_csv (io/output_cases.hpp:489-588) with
+ * the metrics of the current state. */
+ecg_status ecg_write_bubble_summary_csv(ecg_ctx* ctx, const char* path, const ecg_bubble_run* run);
+
+/* ---- measurement -------------------------------------------------------- */
+/* No counterpart in the reference: the FP64 FMA throughput of `device` in
+ * TFLOP/s (independent fma chains at full occupancy, best of five timed
+ * launches), the denominator of the explicit step's FP64 roofline. */
+ecg_status ecg_measure_fp64_peak(int32_t device, double* tflops);
 
 /* ---- adjoint of the explicit step --------------------------------------- */
 /* Vector-Jacobian product of U1 = euler_fv_one_step(U0; dt) with dt held

@@ -385,6 +385,19 @@ struct ReduceData {
 template <std::size_t I, class T>
 inline decltype(auto) get(T&& t) { return std::get<I>(std::forward<T>(t)); }
 
+// Plotfiles are outside the oracle (the hot path never writes them): the
+// writer is a no-op and only the name helper is real.
+inline std::string Concatenate(const std::string& root, int num, int mindigits = 5)
+{
+  char b[32];
+  std::snprintf(b, sizeof(b), "%0*d", mindigits, num);
+  return root + b;
+}
+template <class MF, class Names, class Geom>
+inline void WriteSingleLevelPlotfile(const std::string&, const MF&, const Names&, const Geom&, Real, int)
+{
+}
+
 namespace ParallelDescriptor {
 inline void ReduceRealSum(Real&) {}
 inline void ReduceRealMin(Real&) {}

@@ -1,8 +1,8 @@
 // Reference oracle translation unit.  TEST INFRASTRUCTURE ONLY.
 //
-// Compiles the reference's own euler_compare numerics headers, in the include
-// order of amrex/apps/euler_compare/src/euler_compare_app.cpp:41-62 (minus the
-// app driver and the plotfile/CSV output module), against the single-box AMReX
+// Compiles the reference's own euler_compare numerics and output headers, in
+// the include order of amrex/apps/euler_compare/src/euler_compare_app.cpp:41-62
+// (minus the app driver; plotfiles are a no-op), against the single-box AMReX
 // shim in amrex_shim.hpp and the reference's vendored Eigen.  The extern "C"
 // wrappers below run one reference call on host arrays so tests can compare
 // the CUDA path with the reference's exact arithmetic.
@@ -38,6 +38,7 @@ enum ConservedComponent { Rho = 0, Mx = 1, My = 2, E = 3, NCons = 4 };
 #include "euler_compare/imex/imex_source_map_helpers.hpp"
 #include "euler_compare/imex/imex_pressure_helpers.hpp"
 #include "euler_compare/imex/imex_bdltv20_updates.hpp"
+#include "euler_compare/io/output_cases.hpp"
 
 }  // namespace ecref
 
@@ -478,6 +479,85 @@ int ecref_paper_run(char* out, int len)
   amrex::print_sink() = nullptr;
   if (out && len > 0) std::snprintf(out, static_cast<size_t>(len), "%s", text.c_str());
   return rc;
+}
+
+// The reference's final CSV writers (io/output_cases.hpp:16-216) on a host
+// state: Gresho, Toro, Riemann quadrant or advection blob by the configured
+// problem.  trial_* are the IMEX admissibility run minima of the Gresho file.
+int ecref_write_final_csv(const double* u, int step, double time, const char* path, double trial_rho,
+                          double trial_p, double trial_ie)
+{
+  if (!g_have_cfg) return -1;
+  RunConfig cfg = g_cfg;
+  cfg.final_csv = path;
+  Fabs f(cfg);
+  amrex::MultiFab s(f.ba, f.dm, NCons, 2);
+  load_interior(s, u, cfg.n_cell[0], cfg.n_cell[1]);
+  HighTrialRunDiagnostics h;
+  h.rho_min = trial_rho;
+  h.pressure_min = trial_p;
+  h.internal_energy_min = trial_ie;
+  write_gresho_final_csv(s, f.geom, cfg, step, time, h);
+  write_toro_final_csv(s, f.geom, cfg);
+  write_riemann_quadrant_final_csv(s, f.geom, cfg, step, time);
+  write_advection_blob_final_csv(s, f.geom, cfg, step, time);
+  return 0;
+}
+
+// compute_shock_density_bubble_metrics (io/output_cases.hpp:329-403) after
+// fill_problem_ghosts at `time`: out = rho_min, rho_max, pressure_min,
+// pressure_max, internal_energy_min, centroid_x, centroid_y, area,
+// schlieren_max; returns the nonfinite count.
+int ecref_bubble_metrics(const double* u, double time, double* out)
+{
+  if (!g_have_cfg) return -1;
+  Fabs f(g_cfg);
+  amrex::MultiFab s(f.ba, f.dm, NCons, 2);
+  load_interior(s, u, g_cfg.n_cell[0], g_cfg.n_cell[1]);
+  fill_problem_ghosts(s, f.geom, g_cfg, time);
+  const ShockDensityBubbleMetrics m = compute_shock_density_bubble_metrics(s, f.geom, g_cfg);
+  const double v[9] = {m.rho_min, m.rho_max, m.pressure_min, m.pressure_max, m.internal_energy_min,
+                       m.density_bubble_centroid_x, m.density_bubble_centroid_y, m.density_bubble_area,
+                       m.schlieren_max};
+  for (int k = 0; k < 9; ++k) out[k] = v[k];
+  return m.nonfinite_count;
+}
+
+// write_shock_density_bubble_snapshot (io/output_cases.hpp:422-487) after
+// fill_problem_ghosts at `time`, into `dir`; 0 on success.
+int ecref_bubble_snapshot(const double* u, int step, double time, int index, const char* dir)
+{
+  if (!g_have_cfg) return -1;
+  RunConfig cfg = g_cfg;
+  cfg.shock_density_bubble_snapshot_dir = dir;
+  Fabs f(cfg);
+  amrex::MultiFab s(f.ba, f.dm, NCons, 2);
+  load_interior(s, u, cfg.n_cell[0], cfg.n_cell[1]);
+  fill_problem_ghosts(s, f.geom, cfg, time);
+  return write_shock_density_bubble_snapshot(s, f.geom, cfg, step, time, index) ? 0 : 1;
+}
+
+// write_shock_density_bubble_summary_csv (io/output_cases.hpp:489-588) with
+// the metrics of the state (after fill_problem_ghosts at `time`) and the
+// run-level fields the driver passes.
+int ecref_bubble_summary(const double* u, const char* path, int step, double time, const char* status,
+                         const char* failure, int rejected, double wall, double dt_min, double dt_max,
+                         double dt_mean, const char* snapshot_status, const char* snapshot_dir,
+                         const char* snapshot_times)
+{
+  if (!g_have_cfg) return -1;
+  RunConfig cfg = g_cfg;
+  cfg.final_csv = path;
+  cfg.shock_density_bubble_snapshot_dir = snapshot_dir;
+  cfg.shock_density_bubble_snapshot_times = snapshot_times;
+  Fabs f(cfg);
+  amrex::MultiFab s(f.ba, f.dm, NCons, 2);
+  load_interior(s, u, cfg.n_cell[0], cfg.n_cell[1]);
+  fill_problem_ghosts(s, f.geom, cfg, time);
+  const ShockDensityBubbleMetrics m = compute_shock_density_bubble_metrics(s, f.geom, cfg);
+  write_shock_density_bubble_summary_csv(s, f.geom, cfg, step, time, status, failure, rejected, wall, dt_min, dt_max,
+                                         dt_mean, snapshot_status, m);
+  return 0;
 }
 
 }  // extern "C"

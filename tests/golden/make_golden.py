@@ -230,6 +230,79 @@ def paper_cases(r):
     return out
 
 
+OUT_BASE = {"euler.spatial_order": 2, "euler.slope_limiter": "minmod"}
+IMEX_KEYS = {"euler.method": "imex", "euler.imex_acoustic_startup": 0, "euler.imex_picard_iterations": 2,
+             "euler.imex_solver_tol": "1e-10", "euler.imex_solver_max_iter": 120}
+GRESHO = {"amr.n_cell": "20 16", "geometry.is_periodic": "1 1", "euler.problem": "gresho_vortex",
+          "euler.vortex_center": "0.5 0.5", "euler.mach": 0.1, "euler.pressure": 1.0 / (1.4 * 0.01)}
+OUTPUT_CASES = {
+    # name: (kv, step, time, IMEX admissibility run minima of the Gresho file)
+    "gresho_explicit": (dict(GRESHO, **{"euler.riemann": "xie_am_hllc_p"}), 7, 0.0123, None),
+    "gresho_imex": (dict(GRESHO, **IMEX_KEYS), 3, 0.031, (0.97, 70.9, 177.1)),
+    "toro": ({"amr.n_cell": "24 4", "geometry.prob_hi": "1 0.25", "geometry.is_periodic": "0 1",
+              "euler.problem": "toro1", "euler.riemann": "hllc"}, 11, 0.02, None),
+    "quadrant": ({"amr.n_cell": "16 16", "euler.problem": "riemann_quadrant", "euler.riemann": "hllc",
+                  "geometry.is_periodic": "0 0"}, 5, 0.01, None),
+    "blob": ({"amr.n_cell": "20 16", "euler.problem": "advection_blob", "euler.riemann": "lowmach_hllc",
+              "geometry.is_periodic": "1 1"}, 9, 0.05, None),
+}
+BUBBLE_KV = {"amr.n_cell": "40 10", "geometry.prob_hi": "2 0.5", "euler.problem": "shock_density_bubble_2d",
+             "euler.riemann": "hllc"}
+BUBBLE_RUN = {"step": 4, "time": 0.06, "index": 1, "status": "ok", "failure": "ok", "rejected": 0, "wall": 1.25,
+              "dt_min": 0.011, "dt_max": 0.016, "dt_mean": 0.015, "snapshot_status": "ok",
+              "snapshot_dir": "snaps", "snapshot_times": "0,0.06,0.12"}
+
+
+def perturbed(u, seed):
+    """The problem's initial state with 1 % seeded noise (so every error column is nonzero)."""
+    rng = np.random.default_rng(seed)
+    return u * (1.0 + 0.01 * rng.standard_normal(u.shape))
+
+
+def output_cases(r):
+    """The reference's own writers (io/output_cases.hpp) on seeded states:
+    each final CSV, and the bubble snapshot, metrics and summary."""
+    import tempfile
+
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for k, (name, (kv, step, time, trial)) in enumerate(OUTPUT_CASES.items()):
+            kv = dict(OUT_BASE, **kv)
+            r.configure(kv)
+            u = perturbed(r.initialize(), 100 + k)
+            path = os.path.join(tmp, name + ".csv")
+            r.write_final_csv(u, step, time, path, trial if trial else (float("nan"),) * 3)
+            with open(path) as f:
+                text = f.read()
+            out[name + "_kv"] = np.array(kv_text(kv))
+            out[name + "_u"] = u
+            out[name + "_meta"] = np.array([step, time] + list(trial if trial else (np.nan,) * 3))
+            out[name + "_csv"] = np.array(text)
+        kv = dict(OUT_BASE, **BUBBLE_KV)
+        r.configure(kv)
+        u = perturbed(r.initialize(), 200)
+        b = BUBBLE_RUN
+        r.bubble_snapshot(u, b["step"], b["time"], b["index"], tmp)
+        snap = [f for f in os.listdir(tmp) if f.startswith("snapshot_")]
+        assert len(snap) == 1
+        with open(os.path.join(tmp, snap[0])) as f:
+            out["bubble_snapshot_csv"] = np.array(f.read())
+        out["bubble_snapshot_name"] = np.array(snap[0])
+        m, nf = r.bubble_metrics(u, b["time"])
+        out["bubble_metrics"] = m
+        out["bubble_nonfinite"] = np.array(nf)
+        path = os.path.join(tmp, "summary.csv")
+        r.bubble_summary(u, path, b["step"], b["time"], b["status"], b["failure"], b["rejected"], b["wall"],
+                         b["dt_min"], b["dt_max"], b["dt_mean"], b["snapshot_status"], b["snapshot_dir"],
+                         b["snapshot_times"])
+        with open(path) as f:
+            out["bubble_summary_csv"] = np.array(f.read())
+        out["bubble_kv"] = np.array(kv_text(kv))
+        out["bubble_u"] = u
+        out["bubble_run"] = np.array(json.dumps(b))
+    return out
+
+
 def main():
     r = RefOracle()
     only = sys.argv[1:]
@@ -239,6 +312,8 @@ def main():
         np.savez_compressed(os.path.join(HERE, "sod_400x4.npz"), **sod_case(r))
     if not only or "imex" in only:
         np.savez_compressed(os.path.join(HERE, "imex_cases.npz"), **imex_cases(r))
+    if not only or "output" in only:
+        np.savez_compressed(os.path.join(HERE, "output_cases.npz"), **output_cases(r))
     if not only or "paper" in only:
         with open(os.path.join(HERE, "paper_cases.json"), "w") as f:
             json.dump(paper_cases(r), f, indent=1, sort_keys=True)

@@ -177,6 +177,11 @@ class RefOracle:
             raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference is available")
         lib = C.CDLL(path)
         lib.ecref_paper_run.argtypes = [C.c_char_p, C.c_int]
+        lib.ecref_write_final_csv.argtypes = [_P, C.c_int, _D, C.c_char_p, _D, _D, _D]
+        lib.ecref_bubble_metrics.argtypes = [_P, _D, _P]
+        lib.ecref_bubble_snapshot.argtypes = [_P, C.c_int, _D, C.c_int, C.c_char_p]
+        lib.ecref_bubble_summary.argtypes = [_P, C.c_char_p, C.c_int, _D, C.c_char_p, C.c_char_p, C.c_int, _D, _D,
+                                             _D, _D, C.c_char_p, C.c_char_p, C.c_char_p]
         lib.ecref_paper_run.restype = C.c_int
         lib.ecref_configure.argtypes = [C.c_char_p]
         lib.ecref_last_error.restype = C.c_char_p
@@ -220,6 +225,34 @@ class RefOracle:
             k, _, v = line.partition("=")
             rep[k.strip()] = v.strip()
         return rc, rep
+
+    def write_final_csv(self, u, step, time, path, trial=(float("nan"),) * 3):
+        """The reference's final CSV writer for the configured problem."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        rc = self.lib.ecref_write_final_csv(u.ctypes.data_as(_P), int(step), float(time), os.fsencode(path), *trial)
+        if rc != 0:
+            raise RuntimeError("ecref_write_final_csv failed")
+
+    def bubble_metrics(self, u, time=0.0):
+        """compute_shock_density_bubble_metrics: (nine values, nonfinite count)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.zeros(9)
+        nf = self.lib.ecref_bubble_metrics(u.ctypes.data_as(_P), float(time), out.ctypes.data_as(_P))
+        return out, nf
+
+    def bubble_snapshot(self, u, step, time, index, directory):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if self.lib.ecref_bubble_snapshot(u.ctypes.data_as(_P), int(step), float(time), int(index),
+                                          os.fsencode(directory)) != 0:
+            raise RuntimeError("ecref_bubble_snapshot failed")
+
+    def bubble_summary(self, u, path, step, time, status, failure, rejected, wall, dt_min, dt_max, dt_mean,
+                       snapshot_status, snapshot_dir, snapshot_times):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self.lib.ecref_bubble_summary(u.ctypes.data_as(_P), os.fsencode(path), int(step), float(time), status.encode(),
+                                      failure.encode(), int(rejected), float(wall), float(dt_min), float(dt_max),
+                                      float(dt_mean), snapshot_status.encode(), snapshot_dir.encode(),
+                                      snapshot_times.encode())
 
     def initialize(self):
         u = _state(self.cfg)

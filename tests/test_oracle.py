@@ -1,6 +1,8 @@
 """The CPU restatement (oracle/ecg_oracle.cpp) against the reference's own
 outputs: golden fixtures generated from the reference code, and the live
 reference build (oracle/_ref) where it exists."""
+import os
+
 import numpy as np
 import pytest
 
@@ -182,3 +184,16 @@ def test_paper_fixture_reproduces_live_reference(ref):
         rc, rep = ref.paper_run()
         assert rc == cases[name]["rc"]
         assert rep == cases[name]["report"], name
+
+
+def test_output_fixture_is_the_reference_writers(ref, tmp_path):
+    """tests/golden/output_cases.npz: the reference's Toro and blob writers,
+    run again here, print the committed files."""
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "output_cases.npz"))
+    for name in ("toro", "blob"):
+        ref.configure(str(d[name + "_kv"]))
+        step, time, *trial = d[name + "_meta"]
+        p = str(tmp_path / (name + ".csv"))
+        ref.write_final_csv(d[name + "_u"], int(step), float(time), p, tuple(trial))
+        with open(p) as f:
+            assert f.read() == str(d[name + "_csv"])
