@@ -444,12 +444,10 @@ __device__ __forceinline__ void block_dots(const TV* __restrict__ V, long long n
     for (int i = warp; i < tot; i += NW) {
       double sm = 0.0;
       if (i < nvec) {
+        const TV* pv = V + static_cast<long long>(i) * n + rw.r0 + lane;  // rows at immediate offsets
         TV av[SMALL];
 #pragma unroll
-        for (int k = 0; k < SMALL; ++k) {
-          const int q = rw.r0 + lane + 32 * k;
-          av[k] = q < rw.r1 ? __ldcg(V + static_cast<long long>(i) * n + q) : TV(0);
-        }
+        for (int k = 0; k < SMALL; ++k) av[k] = rw.r0 + lane + 32 * k < rw.r1 ? __ldcg(pv + 32 * k) : TV(0);
 #pragma unroll
         for (int k = 0; k < SMALL; ++k) sm += static_cast<double>(av[k]) * wr[k];
       } else if (i == nvec) {
