@@ -131,6 +131,20 @@ def euler_fv_one_step(ctx, dt, time=0.0):
     return n.value
 
 
+def euler_fv_one_step_host(ctx, u_in, u_out, dt, time=0.0):
+    """One explicit step of a host state (numpy (4, ny, nx) float64 arrays,
+    preferably in pinned memory): upload, step and download pipelined over
+    row bands (ecg_euler_fv_one_step_host).  Returns the degenerate count."""
+    ny, nx = ctx.ny, ctx.nx
+    for a in (u_in, u_out):
+        if a.shape != (4, ny, nx) or a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("host states must be C-contiguous float64 arrays of shape (4, ny, nx)")
+    n = C.c_int32()
+    check(load().ecg_euler_fv_one_step_host(ctx.handle, u_in.ctypes.data, u_out.ctypes.data, 0, 0, nx, nx * ny, dt,
+                                            time, C.byref(n)), "euler_fv_one_step_host", ctx.handle)
+    return n.value
+
+
 def compute_euler_dt(ctx, time=0.0):
     dt = C.c_double()
     check(load().ecg_compute_euler_dt(ctx.handle, time, C.byref(dt)), "compute_euler_dt", ctx.handle)
@@ -203,7 +217,7 @@ def run_bdltv20_paper_t1_s2(ctx, settings):
     driver, and returns its report (abi.PaperResult)."""
     o = paper_options(settings)
     r = abi.PaperResult()
-    check(load().ecg_paper_t1s2_run(ctx.handle, C.byref(o), C.byref(r)), "run_bdltv20_paper_t1_s2", "measure_fp64_peak", ctx.handle)
+    check(load().ecg_paper_t1s2_run(ctx.handle, C.byref(o), C.byref(r)), "run_bdltv20_paper_t1_s2", ctx.handle)
     return r
 
 
@@ -330,10 +344,12 @@ __all__ = [
     "compute_euler_dt",
     "compute_imex_dt",
     "euler_fv_one_step",
+    "euler_fv_one_step_host",
     "euler_imex_bdltv20_o1_source_map_picard_one_step",
     "fill_problem_ghosts",
     "gpu_options",
     "initialize_state",
+    "measure_fp64_peak",
     "read_config",
     "run",
     "run_bdltv20_paper_t1_s2",

@@ -245,6 +245,10 @@ ecg_ctx::~ecg_ctx()
   cudaFree(adj_stats);
   cudaFreeHost(h_stats);
   cudaFreeHost(h_state_stats);
+  for (cudaEvent_t e : band_up) cudaEventDestroy(e);
+  for (cudaEvent_t e : band_done) cudaEventDestroy(e);
+  if (up_stream) cudaStreamDestroy(up_stream);
+  if (down_stream) cudaStreamDestroy(down_stream);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -546,6 +550,135 @@ ecg_status ecg_euler_fv_one_step(ecg_ctx* c, double dt, double time, int32_t* de
   c->fused_valid = false;
   c->fused_pending = true;
   c->fused_slot = ctl.acc_slot;
+  if (degenerate) {
+    if (!fetch_fused(c)) return ECG_ERR_CUDA;
+    *degenerate = c->fused_degenerate;
+  }
+  return ECG_OK;
+}
+
+// euler_fv_one_step on a host-resident box, pipelined over bands of rows:
+// band b+1 is copied to the device on one stream while band b is stepped on
+// the context's stream and the finished bands are copied back on a third,
+// so the two copy directions and the step overlap.  Falls back to upload,
+// step, download in sequence where the step is not the column-strip kernel
+// (exact arithmetic, the HLLC-P tile kernel, exact-Dirichlet rings).
+ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out, int32_t lo_x, int32_t lo_y,
+                                      int64_t jstride, int64_t nstride, double dt, double time, int32_t* degenerate)
+{
+  if (!c || !in || !out) return ECG_ERR_BAD_ARG;
+  const int nx = c->grid.nx, ny = c->grid.ny;
+  if (lo_x > 0 || lo_y > 0 || jstride < nx - lo_x || nstride < jstride * (ny - lo_y)) return ECG_ERR_BAD_ARG;
+  EcgFvParams p = fv_params(c, false);
+  const bool banded = c->opt.arith == ECG_ARITH_FAST && (c->tile_y == 0 || c->tile_y == 2) &&
+                      c->cfg.riemann != ECG_RIEMANN_XIE_AM_HLLC_P && !p.bc.ring && ny >= 32;
+  if (!banded) {
+    ecg_status st = ecg_upload_state(c, in, lo_x, lo_y, jstride, nstride);
+    if (st == ECG_OK) st = ecg_euler_fv_one_step(c, dt, time, degenerate);
+    if (st == ECG_OK) st = ecg_download_state(c, out, lo_x, lo_y, jstride, nstride);
+    return st;
+  }
+  // bands of at least 16 rows, at most 8 of them
+  const int nb = ny / 16 < 8 ? ny / 16 : 8;
+  if (!c->up_stream && !cuda_ok(c, cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking), "stream"))
+    return ECG_ERR_CUDA;
+  if (!c->down_stream && !cuda_ok(c, cudaStreamCreateWithFlags(&c->down_stream, cudaStreamNonBlocking), "stream"))
+    return ECG_ERR_CUDA;
+  while (static_cast<int>(c->band_up.size()) < nb) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (!cuda_ok(c, cudaEventCreateWithFlags(&a, cudaEventDisableTiming), "event") ||
+        !cuda_ok(c, cudaEventCreateWithFlags(&b, cudaEventDisableTiming), "event"))
+      return ECG_ERR_CUDA;
+    c->band_up.push_back(a);
+    c->band_done.push_back(b);
+  }
+  auto row0 = [&](int b) { return static_cast<int>(static_cast<long long>(ny) * b / nb); };
+  const int64_t off = static_cast<int64_t>(-lo_x) + static_cast<int64_t>(-lo_y) * jstride;
+  double* cur = c->cur_state_mut();
+  double* nxt = c->next_state();
+  // the previous call's work on the context's stream (and its read of this
+  // context's state) is ordered before the uploads
+  if (!cuda_ok(c, cudaEventRecord(c->band_done[0], c->stream), "event") ||
+      !cuda_ok(c, cudaStreamWaitEvent(c->up_stream, c->band_done[0], 0), "event"))
+    return ECG_ERR_CUDA;
+  // The four field planes of a band move in one 3D copy (planes at a fixed
+  // stride on both sides); per-plane 2D copies otherwise.  Fewer, larger copy
+  // commands let the two directions share the link better.
+  const bool planes3d = nstride % jstride == 0 && c->grid.plane % c->grid.pitch == 0;
+  auto copy_band = [&](double* dst, long long dpitch, long long dslice, const double* src, long long spitch,
+                       long long sslice, int rows, cudaMemcpyKind kind, cudaStream_t st) -> cudaError_t {
+    if (planes3d) {
+      cudaMemcpy3DParms m;
+      std::memset(&m, 0, sizeof(m));
+      m.srcPtr = make_cudaPitchedPtr(const_cast<double*>(src), sizeof(double) * spitch, sizeof(double) * nx,
+                                     static_cast<size_t>(sslice / spitch));
+      m.dstPtr = make_cudaPitchedPtr(dst, sizeof(double) * dpitch, sizeof(double) * nx,
+                                     static_cast<size_t>(dslice / dpitch));
+      m.extent = make_cudaExtent(sizeof(double) * nx, static_cast<size_t>(rows), 4);
+      m.kind = kind;
+      return cudaMemcpy3DAsync(&m, st);
+    }
+    for (int n = 0; n < 4; ++n) {
+      const cudaError_t e = cudaMemcpy2DAsync(dst + n * dslice, sizeof(double) * dpitch, src + n * sslice,
+                                              sizeof(double) * spitch, sizeof(double) * nx, rows, kind, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  for (int b = 0; b < nb; ++b) {
+    const int r0 = row0(b), r1 = row0(b + 1);
+    if (!cuda_ok(c, copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
+                              in + off + static_cast<int64_t>(r0) * jstride, jstride, nstride, r1 - r0,
+                              cudaMemcpyHostToDevice, c->up_stream),
+                 "upload band"))
+      return ECG_ERR_CUDA;
+    if (!cuda_ok(c, cudaEventRecord(c->band_up[b], c->up_stream), "event")) return ECG_ERR_CUDA;
+  }
+  c->uploaded = true;
+  c->invalidate();
+  if (!c->host_slots_ready) {
+    if (!cuda_ok(c, c->ops->init_stats(c->d_stats, 3, time, c->stream), "init stats")) return ECG_ERR_CUDA;
+    c->host_slots_ready = true;
+    c->host_step = 0;
+  }
+  EcgDtCtl ctl;
+  std::memset(&ctl, 0, sizeof(ctl));
+  ctl.dt = dt;
+  ctl.time = time;
+  ctl.count_degenerate = c->cfg.riemann != ECG_RIEMANN_RUSANOV;
+  ctl.read_slot = static_cast<int>(c->host_step % 3);
+  ctl.acc_slot = static_cast<int>((c->host_step + 1) % 3);
+  ctl.reset_slot = static_cast<int>((c->host_step + 2) % 3);
+  for (int b = 0; b < nb; ++b) {
+    // rows r0-2 .. r1+1 are read: this band's upload and the next one's
+    if (!cuda_ok(c, cudaStreamWaitEvent(c->stream, c->band_up[b], 0), "event")) return ECG_ERR_CUDA;
+    if (b + 1 < nb && !cuda_ok(c, cudaStreamWaitEvent(c->stream, c->band_up[b + 1], 0), "event")) return ECG_ERR_CUDA;
+    p.row_lo = row0(b);
+    p.row_hi = row0(b + 1);
+    if (!cuda_ok(c, c->ops->fv_step(p, cur, nxt, c->d_stats, ctl, c->tile_y, c->stream), "fv_step band"))
+      return ECG_ERR_CUDA;
+    if (!cuda_ok(c, cudaEventRecord(c->band_done[b], c->stream), "event") ||
+        !cuda_ok(c, cudaStreamWaitEvent(c->down_stream, c->band_done[b], 0), "event"))
+      return ECG_ERR_CUDA;
+    const int r0 = row0(b), r1 = row0(b + 1);
+    if (!cuda_ok(c, copy_band(out + off + static_cast<int64_t>(r0) * jstride, jstride, nstride,
+                              nxt + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane, r1 - r0,
+                              cudaMemcpyDeviceToHost, c->down_stream),
+                 "download band"))
+      return ECG_ERR_CUDA;
+  }
+  c->cur ^= 1;
+  ++c->host_step;
+  c->state_stats_valid = false;
+  c->fused_valid = false;
+  c->fused_pending = true;
+  c->fused_slot = ctl.acc_slot;
+  // the caller owns `out` on return; the context's stream waits for the
+  // copies before it touches the state again
+  if (!cuda_ok(c, cudaEventRecord(c->band_up[0], c->down_stream), "event") ||
+      !cuda_ok(c, cudaStreamWaitEvent(c->stream, c->band_up[0], 0), "event") ||
+      !cuda_ok(c, cudaStreamSynchronize(c->down_stream), "sync"))
+    return ECG_ERR_CUDA;
   if (degenerate) {
     if (!fetch_fused(c)) return ECG_ERR_CUDA;
     *degenerate = c->fused_degenerate;

@@ -24,6 +24,10 @@ struct ecg_ctx {
   int tile_y = 16;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // pipelined host step (ecg_euler_fv_one_step_host): copy streams and one
+  // event per band for the upload and for the step
+  cudaStream_t up_stream = nullptr, down_stream = nullptr;
+  std::vector<cudaEvent_t> band_up, band_done;
 
   double* d_state[2] = {nullptr, nullptr};  // double buffer, 4 planes each
   int cur = 0;

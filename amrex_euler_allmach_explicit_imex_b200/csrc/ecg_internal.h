@@ -75,6 +75,7 @@ struct EcgFvParams {
   int order, limiter, riemann;
   int march_rows;            // rows per warp of the column-strip kernel (0: sized to fill one wave)
   int sm_count;              // SMs of the device (0: 148)
+  int row_lo, row_hi;        // column-strip kernel: update rows [row_lo, row_hi) only (row_hi 0: all rows)
   int pad;
 };
 

@@ -127,7 +127,8 @@ __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* 
   const bool cell_ok = inner && x < nx;                 // that cell is in the domain
   const bool xface = lane >= 2 && lane <= 2 + kCells;   // its x-face on the left belongs to the strip
   const int xs = x < 0 ? 0 : (x < nx ? x : nx - 1);     // in-bounds column for the old-state reload
-  const int jend = j0 + H < ny ? j0 + H : ny;
+  const int rhi = P.row_hi > 0 && P.row_hi < ny ? P.row_hi : ny;  // end of the band of rows being updated
+  const int jend = j0 + H < rhi ? j0 + H : rhi;
 
   // ---- prologue: rows j0-2 .. j0+1, y-slopes of rows j0-1 and j0, the y-face below row j0 ----
   Prim q_m2 = fast::to_prim_f(load_cell(P, u, x, j0 - 2), g);
@@ -215,7 +216,7 @@ fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __res
   __shared__ BlockRed<WPB * 32> red;
   const int strip = blockIdx.x * WPB + (threadIdx.x >> 5);
   const int c0 = strip * kCells;
-  const int j0 = blockIdx.y * H;
+  const int j0 = (P.row_hi > 0 ? P.row_lo : 0) + blockIdx.y * H;
 
   double dt;
   if (!step_control(stats, ctl, dt)) return;
@@ -235,6 +236,11 @@ cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgS
 {
   constexpr int WPB = 4;
   const int strips = (p.g.nx + kCells - 1) / kCells;
+  // a band of rows (the pipelined host step) or the whole grid
+  const int rlo = p.row_hi > 0 ? p.row_lo : 0;
+  const int rhi = p.row_hi > 0 && p.row_hi < p.g.ny ? p.row_hi : p.g.ny;
+  const int rows = rhi - rlo;
+  if (rows <= 0) return cudaSuccess;
   int H = p.march_rows;
   if (H <= 0) {
     static int blocks_per_sm = 0;
@@ -247,10 +253,10 @@ cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgS
     }
     const long long slots = static_cast<long long>(p.sm_count > 0 ? p.sm_count : 148) * blocks_per_sm * WPB;
     const long long per_col = slots / strips;  // warps available per strip column
-    H = per_col > 0 ? static_cast<int>((p.g.ny + per_col - 1) / per_col) : p.g.ny;
+    H = per_col > 0 ? static_cast<int>((rows + per_col - 1) / per_col) : rows;
     if (H < 8) H = 8;
   }
-  const dim3 grid((strips + WPB - 1) / WPB, (p.g.ny + H - 1) / H);
+  const dim3 grid((strips + WPB - 1) / WPB, (rows + H - 1) / H);
   fv_march_kernel<RK, LIM, WPB, PAIR><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl, H);
   return cudaGetLastError();
 }

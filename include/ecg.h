@@ -376,6 +376,17 @@ ecg_status ecg_synchronize(ecg_ctx* ctx);
  * count_hllc_degenerate_star_states value (explicit_update.hpp:2-56) through
  * hllc_degenerate_count when non-NULL. */
 ecg_status ecg_euler_fv_one_step(ecg_ctx* ctx, double dt, double time, int32_t* hllc_degenerate_count);
+/* euler_fv_one_step on a HOST box (the Array4 description of
+ * ecg_upload_state for `in` and `out`, which may be the same array): the
+ * upload, the step and the download in one call, pipelined over bands of
+ * rows so that band b+1 crosses to the device while band b is stepped and
+ * finished bands cross back.  Pinned host memory lets the copies overlap.
+ * The context's state becomes the new state, and its fused CFL / diagnostic
+ * reductions are those of `out`.  No counterpart in the reference (a drop-in
+ * for its host-MultiFab call sequence upload -> euler_fv_one_step ->
+ * download). */
+ecg_status ecg_euler_fv_one_step_host(ecg_ctx* ctx, const double* in, double* out, int32_t lo_x, int32_t lo_y,
+                                      int64_t jstride, int64_t nstride, double dt, double time, int32_t* degenerate);
 /* compute_euler_dt (numerics/diagnostic_metrics_timestep.hpp:227-260). */
 ecg_status ecg_compute_euler_dt(ecg_ctx* ctx, double time, double* dt);
 /* compute_imex_dt (numerics/diagnostic_metrics_timestep.hpp:272-326). */

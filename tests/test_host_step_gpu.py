@@ -1,0 +1,64 @@
+"""ecg_euler_fv_one_step_host: the upload, step and download of a host state
+in one call, pipelined over row bands, against the device-resident step on
+the same state.  Band edges are strip edges of the column-strip kernel, whose
+y-faces there go through the one-face flux: fast arithmetic agrees to 1e-12
+per step, as between any two strip partitions."""
+import numpy as np
+import pytest
+
+from amrex_euler_allmach_explicit_imex_b200 import api
+from amrex_euler_allmach_explicit_imex_b200.config import read_config
+from tests import golden_io
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "bubble": "amr.n_cell=320 80\ngeometry.prob_hi=2 0.5\neuler.problem=shock_density_bubble_2d\neuler.riemann=hllc\n",
+    "toro_periodic_y": "amr.n_cell=200 96\ngeometry.prob_hi=1 0.48\neuler.problem=toro1\neuler.riemann=lowmach_hllc\n"
+                       "geometry.is_periodic=0 1\n",
+    "gresho_hllcp": "amr.n_cell=96 96\ngeometry.is_periodic=1 1\neuler.problem=gresho_vortex\neuler.vortex_center=0.5 0.5\n"
+                    "euler.riemann=xie_am_hllc_p\n",
+}
+
+
+@pytest.mark.parametrize("arith", ["fast", "exact"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_host_step_matches_device_step(gpu, name, arith):
+    cfg = read_config(CASES[name]).cfg
+    with api.Context(cfg, arith=arith) as ctx:
+        api.initialize_state(ctx)
+        u0 = ctx.download()
+        t, states, degs = 0.0, [], []
+        for _ in range(3):
+            dt = api.compute_euler_dt(ctx, t)
+            degs.append(api.euler_fv_one_step(ctx, dt, t))
+            states.append(ctx.download())
+            t += dt
+    with api.Context(cfg, arith=arith) as ctx:
+        a = np.ascontiguousarray(u0)
+        b = np.empty_like(a)
+        ctx.upload(a)
+        t = 0.0
+        for k in range(3):
+            dt = api.compute_euler_dt(ctx, t)  # the fused reduction of the previous host step
+            deg = api.euler_fv_one_step_host(ctx, a, b, dt, t)
+            tol = 0.0 if arith == "exact" else 1e-12 * (k + 1)
+            assert golden_io.state_rel_err(b, states[k]) <= tol
+            assert abs(deg - degs[k]) <= (0 if arith == "exact" else 2)
+            np.testing.assert_array_equal(ctx.download(), b)
+            a, b = b, a
+            t += dt
+
+
+def test_host_step_in_place(gpu):
+    cfg = read_config(CASES["bubble"]).cfg
+    with api.Context(cfg) as ctx:
+        api.initialize_state(ctx)
+        u = np.ascontiguousarray(ctx.download())
+        ref = u.copy()
+        dt = api.compute_euler_dt(ctx)
+        api.euler_fv_one_step(ctx, dt)
+        want = ctx.download()
+        ctx.upload(ref)
+        api.euler_fv_one_step_host(ctx, u, u, dt)
+        assert golden_io.state_rel_err(u, want) <= 1e-12
