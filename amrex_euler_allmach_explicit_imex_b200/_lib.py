@@ -36,6 +36,10 @@ SIGNATURES = {
     "ecg_initialize_state": (C.c_int, [_CTX]),
     "ecg_paper_t1s2_run": (C.c_int, [_CTX, C.POINTER(abi.PaperOptions), C.POINTER(abi.PaperResult)]),
     "ecg_measure_fp64_peak": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
+    "ecg_create_slab": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(abi.RunConfig), C.POINTER(abi.GpuOptions), C.c_int32,
+                                  C.c_int32, C.c_int32, C.c_int32]),
+    "ecg_slab_bind_halo": (C.c_int, [_CTX, C.c_void_p, C.c_void_p]),
+    "ecg_slab_pack": (C.c_int, [_CTX, C.c_void_p, C.c_void_p]),
     "ecg_euler_fv_one_step_host": (C.c_int, [_CTX, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
                                              C.c_double, C.c_double, C.POINTER(C.c_int32)]),
     "ecg_write_final_csv": (C.c_int, [_CTX, C.c_char_p, C.POINTER(abi.OutputInfo)]),

@@ -56,7 +56,9 @@ class Context:
     """One device-resident state (the MultiFab of the reference) and its
     configuration; owns all device buffers."""
 
-    def __init__(self, cfg, **gpu):
+    def __init__(self, cfg, slab=None, **gpu):
+        """slab=(x0, x1, halo_lo, halo_hi): columns [x0, x1) of the grid, with
+        ghost columns from neighbour slabs on the halo sides (ecg_create_slab)."""
         lib = load()
         if isinstance(cfg, RunSettings):
             cfg = cfg.cfg
@@ -65,9 +67,27 @@ class Context:
         self.cfg = cfg.copy()
         self.opt = gpu_options(**gpu)
         h = C.c_void_p()
-        check(lib.ecg_create(C.byref(h), C.byref(self.cfg), C.byref(self.opt)), "ecg_create")
+        if slab is None:
+            check(lib.ecg_create(C.byref(h), C.byref(self.cfg), C.byref(self.opt)), "ecg_create")
+            self.nx = self.cfg.n_cell[0]
+        else:
+            x0, x1, hlo, hhi = slab
+            check(lib.ecg_create_slab(C.byref(h), C.byref(self.cfg), C.byref(self.opt), int(x0), int(x1), int(bool(hlo)),
+                                      int(bool(hhi))), "ecg_create_slab")
+            self.nx = int(x1) - int(x0)
         self._h = h
-        self.nx, self.ny = self.cfg.n_cell[0], self.cfg.n_cell[1]
+        self.ny = self.cfg.n_cell[1]
+
+    def bind_halo(self, lo, hi):
+        """Device halo blocks (torch tensors of 8 ny float64, or None) the
+        steps of a slab read (ecg_slab_bind_halo)."""
+        check(load().ecg_slab_bind_halo(self._h, None if lo is None else lo.data_ptr(),
+                                        None if hi is None else hi.data_ptr()), "ecg_slab_bind_halo", self._h)
+
+    def pack(self, lo, hi):
+        """The slab's edge columns into device blocks (ecg_slab_pack)."""
+        check(load().ecg_slab_pack(self._h, None if lo is None else lo.data_ptr(), None if hi is None else hi.data_ptr()),
+              "ecg_slab_pack", self._h)
 
     @property
     def handle(self):

@@ -162,6 +162,10 @@ EcgFvParams fv_params(ecg_ctx* c, bool imex_policy)
   p.riemann = c->cfg.riemann;
   p.march_rows = c->opt.tile_x;
   p.sm_count = c->num_sms;
+  if (c->halo_lo) p.bc.x_lo = BC_HALO;
+  if (c->halo_hi) p.bc.x_hi = BC_HALO;
+  p.halo_lo = c->d_halo_lo;
+  p.halo_hi = c->d_halo_hi;
   return p;
 }
 
@@ -570,7 +574,7 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
   const int nx = c->grid.nx, ny = c->grid.ny;
   if (lo_x > 0 || lo_y > 0 || jstride < nx - lo_x || nstride < jstride * (ny - lo_y)) return ECG_ERR_BAD_ARG;
   EcgFvParams p = fv_params(c, false);
-  const bool banded = c->opt.arith == ECG_ARITH_FAST && (c->tile_y == 0 || c->tile_y == 2) &&
+  const bool banded = c->opt.arith == ECG_ARITH_FAST && (c->tile_y == 0 || c->tile_y == 2) && !c->slab() &&
                       c->cfg.riemann != ECG_RIEMANN_XIE_AM_HLLC_P && !p.bc.ring && ny >= 32;
   if (!banded) {
     ecg_status st = ecg_upload_state(c, in, lo_x, lo_y, jstride, nstride);
@@ -882,8 +886,91 @@ ecg_status ecg_run(ecg_ctx* c, int32_t max_step, double stop_time, ecg_run_resul
 {
   if (!c || !out) return ECG_ERR_BAD_ARG;
   if (!c->uploaded) return ECG_ERR_NOT_READY;
+  if (c->slab()) {
+    c->err = "a slab needs its halo exchanged every step: step it with ecg_euler_fv_one_step";
+    return ECG_ERR_UNSUPPORTED;
+  }
   if (c->cfg.method == ECG_METHOD_IMEX) return imex_run(c, max_step, stop_time, out);
   return run_explicit(c, max_step, stop_time, out);
+}
+
+// ---- slabs of a grid split along x ------------------------------------------
+
+namespace {
+// Edge columns of a slab into the halo layout (4 planes x ny rows x 2):
+// lo <- columns 0, 1; hi <- columns nx-2, nx-1.
+__global__ void slab_pack_kernel(const double* __restrict__ u, long long pitch, long long plane, int nx, int ny,
+                                 double* __restrict__ lo, double* __restrict__ hi)
+{
+  const long long n = 4LL * ny * 2;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(t & 1);
+    const long long fj = t >> 1;  // field * ny + row
+    const int f = static_cast<int>(fj / ny), j = static_cast<int>(fj - static_cast<long long>(f) * ny);
+    const double* row = u + f * plane + j * pitch;
+    if (lo) lo[t] = row[k];
+    if (hi) hi[t] = row[nx - 2 + k];
+  }
+}
+}  // namespace
+
+ecg_status ecg_create_slab(ecg_ctx** out, const ecg_run_config* cfg, const ecg_gpu_options* opt, int32_t x0,
+                           int32_t x1, int32_t halo_lo, int32_t halo_hi)
+{
+  if (!out || !cfg) return ECG_ERR_BAD_ARG;
+  *out = nullptr;
+  const int nx = cfg->n_cell[0];
+  if (x0 < 0 || x1 > nx || x1 - x0 < 2 || !(cfg->prob_hi[0] > cfg->prob_lo[0])) return ECG_ERR_BAD_ARG;
+  if (halo_lo || halo_hi) {
+    if (cfg->method == ECG_METHOD_IMEX) return ECG_ERR_UNSUPPORTED;
+    EcgBc bc;
+    EcgProblem pr;
+    std::memset(&bc, 0, sizeof(bc));
+    make_bc(*cfg, false, bc, pr);
+    if (bc.ring) return ECG_ERR_UNSUPPORTED;  // exact-state Dirichlet rings cover the whole grid
+  }
+  // the global cell size (AMReX Geometry: (hi - lo) / n) and the slab's origin
+  const double dx = (cfg->prob_hi[0] - cfg->prob_lo[0]) / static_cast<double>(nx);
+  ecg_run_config local = *cfg;
+  local.n_cell[0] = x1 - x0;
+  local.prob_lo[0] = cfg->prob_lo[0] + static_cast<double>(x0) * dx;
+  local.prob_hi[0] = cfg->prob_lo[0] + static_cast<double>(x1) * dx;
+  const ecg_status st = ecg_create(out, &local, opt);
+  if (st != ECG_OK) return st;
+  ecg_ctx* c = *out;
+  // the problem keeps the whole grid's extent (periodic wraps, exact states);
+  // the slab's cells keep the whole grid's dx bit for bit
+  c->cfg.prob_lo[0] = cfg->prob_lo[0];
+  c->cfg.prob_hi[0] = cfg->prob_hi[0];
+  c->grid.dx = dx;
+  c->grid.inv_dx = 1.0 / dx;
+  c->grid.plo_x = local.prob_lo[0];
+  c->halo_lo = halo_lo != 0;
+  c->halo_hi = halo_hi != 0;
+  c->slab_x0 = x0;
+  return ECG_OK;
+}
+
+ecg_status ecg_slab_bind_halo(ecg_ctx* c, const double* lo, const double* hi)
+{
+  if (!c) return ECG_ERR_BAD_ARG;
+  if ((c->halo_lo && !lo) || (c->halo_hi && !hi)) return ECG_ERR_BAD_ARG;
+  c->d_halo_lo = lo;
+  c->d_halo_hi = hi;
+  c->invalidate();
+  return ECG_OK;
+}
+
+ecg_status ecg_slab_pack(ecg_ctx* c, double* lo, double* hi)
+{
+  if (!c || (!lo && !hi)) return ECG_ERR_BAD_ARG;
+  if (!c->uploaded) return ECG_ERR_NOT_READY;
+  const long long n = 8LL * c->grid.ny;
+  const int blocks = static_cast<int>((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184);
+  slab_pack_kernel<<<blocks, 256, 0, c->stream>>>(c->cur_state(), c->grid.pitch, c->grid.plane, c->grid.nx,
+                                                  c->grid.ny, lo, hi);
+  return cuda_ok(c, cudaGetLastError(), "slab pack") ? ECG_OK : ECG_ERR_CUDA;
 }
 
 }  // extern "C"

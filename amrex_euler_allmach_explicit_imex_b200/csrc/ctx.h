@@ -60,6 +60,13 @@ struct ecg_ctx {
   };
   std::vector<Graph> graphs;
 
+  // slab of a grid split along x (ecg_create_slab): x sides whose ghost
+  // columns come from the neighbour slabs, and the caller's halo blocks
+  bool halo_lo = false, halo_hi = false;
+  int slab_x0 = 0;
+  const double* d_halo_lo = nullptr;
+  const double* d_halo_hi = nullptr;
+  bool slab() const { return halo_lo || halo_hi; }
   EcgImexState* imex = nullptr;
   EcgOutput* out = nullptr;  // output writers' buffers (output.cu)
   // adjoint workspace (adjoint.cu): primitive gradients, one stats record

@@ -11,7 +11,8 @@ enum EcgBcKind : int {
   BC_PERIODIC = 0,  // FillBoundary(periodicity): wrap
   BC_CLAMP = 1,     // outflow: nearest valid cell
   BC_REFLECT = 2,   // shock-bubble bottom wall: mirror row, negate my
-  BC_CONST = 3      // shock-bubble inflow: fixed post-shock conserved state
+  BC_CONST = 3,     // shock-bubble inflow: fixed post-shock conserved state
+  BC_HALO = 4       // x side of a slab: ghost columns from the neighbour slab (EcgFvParams::halo)
 };
 
 struct EcgBc {
@@ -77,6 +78,10 @@ struct EcgFvParams {
   int sm_count;              // SMs of the device (0: 148)
   int row_lo, row_hi;        // column-strip kernel: update rows [row_lo, row_hi) only (row_hi 0: all rows)
   int pad;
+  // BC_HALO sides: columns -2, -1 (halo_lo) and nx, nx+1 (halo_hi), each
+  // block 4 planes of ny rows x 2 columns
+  const double* halo_lo;
+  const double* halo_hi;
 };
 
 // Per-step reduction record.  Keys are order-preserving integer images of

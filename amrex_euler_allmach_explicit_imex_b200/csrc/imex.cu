@@ -187,6 +187,10 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
   if (!c || !out) return ECG_ERR_BAD_ARG;
   if (!c->uploaded) return ECG_ERR_NOT_READY;
   if (c->cfg.spatial_order != 2) return ECG_ERR_UNSUPPORTED;
+  if (c->slab()) {
+    c->err = "the IMEX pressure system couples the whole grid: no slab contexts";
+    return ECG_ERR_UNSUPPORTED;
+  }
   if (c->cfg.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122) {
     c->err = "the Mach 1.22 shock-bubble configuration runs the explicit method only";
     return ECG_ERR_UNSUPPORTED;

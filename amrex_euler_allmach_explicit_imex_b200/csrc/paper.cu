@@ -534,6 +534,10 @@ extern "C" ecg_status ecg_paper_t1s2_run(ecg_ctx* c, const ecg_paper_options* op
 {
   if (!c || !opts || !out) return ECG_ERR_BAD_ARG;
   std::memset(out, 0, sizeof(*out));
+  if (c->slab()) {
+    c->err = "the direct T1/S2 driver runs on the whole grid: no slab contexts";
+    return ECG_ERR_UNSUPPORTED;
+  }
   const ecg_run_config& cfg = c->cfg;
   std::string why;
   if (!mode_ok(cfg, *opts, why)) {

@@ -51,12 +51,16 @@ __device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __
     const long long pl = P.ring_plane;
     return Cons{P.ring[o], P.ring[o + pl], P.ring[o + 2 * pl], P.ring[o + 3 * pl]};
   }
+  int hs = -1;  // halo column of a slab side: 0, 1 left (x = -2, -1), 2, 3 right (x = nx, nx + 1)
   if (i < 0) {
-    if (P.bc.x_lo == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
-    i = P.bc.x_lo == BC_PERIODIC ? wrapi(i, nx) : 0;
+    if (P.bc.x_lo == BC_HALO) hs = i < -2 ? 0 : i + 2;
+    else if (P.bc.x_lo == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+    else i = P.bc.x_lo == BC_PERIODIC ? wrapi(i, nx) : 0;
   } else if (i >= nx) {
-    if (P.bc.x_hi == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
-    i = P.bc.x_hi == BC_PERIODIC ? wrapi(i, nx) : nx - 1;
+    // strips past the last column read cells beyond the halo; they feed no face of the slab
+    if (P.bc.x_hi == BC_HALO) hs = i - nx > 1 ? 3 : 2 + (i - nx);
+    else if (P.bc.x_hi == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+    else i = P.bc.x_hi == BC_PERIODIC ? wrapi(i, nx) : nx - 1;
   }
   bool flip = false;
   if (j < 0) {
@@ -81,6 +85,15 @@ __device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __
     } else {
       j = ny - 1;
     }
+  }
+  if (hs >= 0) {
+    // the neighbour slab's cell, after the y policy (a corner ghost is the
+    // y-mapped row of the halo column, as in the undivided grid)
+    const long long fs = 2LL * ny;
+    const double* h = (hs < 2 ? P.halo_lo : P.halo_hi) + static_cast<long long>(j) * 2 + (hs & 1);
+    Cons c{h[0], h[fs], h[2 * fs], h[3 * fs]};
+    if (flip) c.my = -c.my;
+    return c;
   }
   const long long o = static_cast<long long>(j) * P.g.pitch + i;
   const long long pl = P.g.plane;

@@ -463,6 +463,25 @@ ecg_status ecg_output_wait(ecg_ctx* ctx, int32_t* failed);
  * the metrics of the current state. */
 ecg_status ecg_write_bubble_summary_csv(ecg_ctx* ctx, const char* path, const ecg_bubble_run* run);
 
+/* ---- slabs of a grid split along x (several GPUs) ------------------------ */
+/* No counterpart in the reference (it runs one box on one process).  A slab
+ * context holds columns [x0, x1) of the grid `cfg` describes, with the whole
+ * grid's dx bit for bit and the whole grid's problem definition; halo_lo /
+ * halo_hi mark the x sides whose two ghost columns are a neighbour slab's edge
+ * columns (periodic x: every side).  Explicit method only, and no
+ * exact-state Dirichlet rings (ECG_ERR_UNSUPPORTED).  Halo blocks are device
+ * buffers of 8 ny doubles: 4 planes (rho, mx, my, E) of ny rows x 2 columns,
+ * columns in increasing x.  A step reads the blocks bound last; y ghosts of
+ * the halo columns follow the y policy, as in the undivided grid. */
+ecg_status ecg_create_slab(ecg_ctx** out, const ecg_run_config* cfg, const ecg_gpu_options* opt, int32_t x0,
+                           int32_t x1, int32_t halo_lo, int32_t halo_hi);
+/* Binds the halo blocks the steps read: lo = columns -2, -1; hi = nx, nx+1. */
+ecg_status ecg_slab_bind_halo(ecg_ctx* ctx, const double* lo, const double* hi);
+/* Writes the slab's edge columns of the current state, on the context's
+ * stream: lo <- columns 0, 1 (the left neighbour's hi halo), hi <- columns
+ * nx-2, nx-1 (the right neighbour's lo halo).  Either may be NULL. */
+ecg_status ecg_slab_pack(ecg_ctx* ctx, double* lo, double* hi);
+
 /* ---- measurement -------------------------------------------------------- */
 /* No counterpart in the reference: the FP64 FMA throughput of `device` in
  * TFLOP/s (independent fma chains at full occupancy, best of five timed
