@@ -374,6 +374,7 @@ struct SolveState {
   int best_it;     // index of the iterate returned
   double best_linf;
   double r0_linf;  // infinity norm of b - A x0
+  double b_linf;   // infinity norm of b
   int converged, breakdown, nonfinite, timeout;
   int restart;     // mixed: the recurrence residual fell by inner_rtol
 };
@@ -631,6 +632,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   st.best_it = 0;
   st.best_linf = __builtin_huge_val();
   st.r0_linf = __builtin_huge_val();
+  st.b_linf = 0.0;
   st.converged = st.breakdown = st.nonfinite = st.timeout = st.restart = 0;
   double beta = 0.0;
 
@@ -652,6 +654,8 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   const double r0inf = grid_max_redundant(a.part, ld, 1, S.scratch);
   grid_reduce_redundant(a.part + 2, ld, 1, S.red, S.scratch);
   beta = sqrt(S.red[0]);
+  st.r0_linf = r0inf;
+  st.b_linf = bn_raw;
   const double bn = bn_raw > 1.0 ? bn_raw : 1.0;
   const double rtarget = restart_rtol > 0.0 ? restart_rtol * r0inf : -1.0;
   bool stop = false;
@@ -660,7 +664,6 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     stop = true;
   } else {
     st.best_linf = r0inf;  // update_best(initial_guess, 0)
-    st.r0_linf = r0inf;
     if (r0inf <= tol || r0inf / bn <= tol) {
       st.converged = 1;
       stop = true;
@@ -847,6 +850,8 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
     out.timeout = st.timeout;
     out.residual_linf = st.best_linf;
     out.inner_iterations = st.it;
+    out.initial_linf = st.r0_linf;
+    out.b_linf = st.b_linf;
   } else {
     // Cycles of the FP32-basis solve; each opens with the true FP64 residual
     // of the current iterate (x0, then x) and the reference's stopping rule.
@@ -861,6 +866,10 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
       const int kin = per_cycle < left ? per_cycle : left;
       st = krylov<float>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol, gen,
                          sh);
+      if (cycles == 0) {
+        out.initial_linf = st.r0_linf;
+        out.b_linf = st.b_linf;
+      }
       ++cycles;
       out.iterations = total + st.best_it;
       total += st.it;
@@ -882,6 +891,35 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
     out.refinements = cycles;
   }
   out.relative_residual_linf = 0.0;
+  // ---- the returned iterate's true residual ||A x - b||inf, ||b||inf (one
+  // sweep after x is complete; the host reads them with the result) ----
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  out.final_linf = out.final_b_linf = nan;
+  if (!out.timeout && grid_sync(a.bar, gen, a.spin_limit)) {
+    const Rows rw = own_rows(a.n);
+    const Smem S = carve(sh, a.m);
+    double* part_row = a.part + static_cast<long long>(blockIdx.x) * a.ld;
+    double rmax = 0.0, bmax = 0.0;
+    for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
+      const int qq[1] = {q};
+      double ax[1];
+      apply_rows<double, 1>(a.op, a.x, qq, ax);
+      rmax = nanmax(rmax, fabs(ax[0] - a.b[q]));
+      bmax = nanmax(bmax, fabs(a.b[q]));
+    }
+    block_max_partial(rmax, part_row, 0, S.scratch);
+    block_max_partial(bmax, part_row, 1, S.scratch);
+    if (grid_sync(a.bar, gen, a.spin_limit)) {
+      if (blockIdx.x == 0) {
+        out.final_linf = grid_max_redundant(a.part, a.ld, 0, S.scratch);
+        out.final_b_linf = grid_max_redundant(a.part, a.ld, 1, S.scratch);
+      }
+    } else {
+      out.timeout = 1;
+    }
+  } else {
+    out.timeout = 1;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.res = out;
 }
 

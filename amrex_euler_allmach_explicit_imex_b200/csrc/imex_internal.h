@@ -95,6 +95,10 @@ struct EcgGmresResult {
   int pad;
   double residual_linf;
   double relative_residual_linf;
+  // true residuals, as pressure_residual computes them: ||A x0 - b||inf and
+  // ||b||inf at the start, ||A x - b||inf and ||b||inf of the returned x
+  // (NaN when nonfinite; the final pair is NaN after a timeout)
+  double initial_linf, b_linf, final_linf, final_b_linf;
 };
 
 struct EcgGmresWork;  // gmres.cu
