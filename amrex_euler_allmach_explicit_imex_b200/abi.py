@@ -73,6 +73,7 @@ class GpuOptions(C.Structure):
         ("mixed_max_refinements", C.c_int32),
         ("tile_x", C.c_int32),
         ("tile_y", C.c_int32),
+        ("mixed_reorth", C.c_int32),
         ("stream", C.c_void_p),
     ]
 

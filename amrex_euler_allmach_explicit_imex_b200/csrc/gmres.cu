@@ -74,6 +74,7 @@ struct GmresArgs {
   int inner_max;      // mixed: iterations per cycle
   double inner_rtol;  // mixed: restart when the recurrence residual fell by this factor
   int max_refine;     // mixed: cycles
+  int reorth;         // mixed: DGKS test of the FP32-basis cycles, 1 as the FP64 solve, 0 severe cancellation only
   long long spin_limit;
 };
 
@@ -741,7 +742,12 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     }
     __syncthreads();
     double nn2 = sw - dsum;
-    if (!(nn2 >= 0.5 * sw)) {
+    // DGKS: a second pass when ||w'||^2 < eta ||w||^2.  The FP32-basis cycles
+    // may take it only under severe cancellation: their basis rounding
+    // (2^-24) already bounds orthogonality far above what the second pass
+    // restores, and a cycle only has to reduce its residual by inner_rtol.
+    const double eta = (sizeof(TV) == 8 || a.reorth) ? 0.5 : 1.0e-6;
+    if (!(nn2 >= eta * sw)) {
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
       if (wide) sweep_combine<TV, true, 2>(rw, V, n, S.coef, j + 1, w, w);
       else sweep_combine<TV, true, 1>(rw, V, n, S.coef, j + 1, w, w);
@@ -1036,7 +1042,7 @@ void gmres_work_destroy(EcgGmresWork* w)
 
 cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
                         int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
-                        EcgGmresResult* out, cudaStream_t s)
+                        int reorth, EcgGmresResult* out, cudaStream_t s)
 {
   if (mixed != w->mixed) return cudaErrorInvalidValue;  // the basis is allocated for one precision
   GmresArgs a;
@@ -1062,6 +1068,7 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.inner_max = inner_max_iter < a.max_iter ? inner_max_iter : a.max_iter;  // <= 0: no per-cycle limit
   a.inner_rtol = inner_rtol;
   a.max_refine = max_refine;
+  a.reorth = reorth;
   a.spin_limit = 1LL << 25;  // ~2 s of polling before a barrier gives up
   cudaError_t e = cudaMemsetAsync(w->bar, 0, sizeof(GridBar), s);
   if (e != cudaSuccess) return e;

@@ -274,7 +274,7 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     EcgGmresResult g;
     if (!ecgi::cuda_ok(c, gmres_solve(im->gw, op, im->rhs, im->p, im->x, c->cfg.imex_solver_max_iter, tol, mixed,
                                       c->opt.mixed_inner_max_iter, c->opt.mixed_inner_rtol,
-                                      c->opt.mixed_max_refinements, &g, s),
+                                      c->opt.mixed_max_refinements, c->opt.mixed_reorth, &g, s),
                        "gmres"))
       return ECG_ERR_CUDA;
     if (g.timeout) {

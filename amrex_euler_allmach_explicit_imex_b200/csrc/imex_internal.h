@@ -110,7 +110,7 @@ void gmres_work_destroy(EcgGmresWork* w);
 // mixed: FP32 inner GMRES inside FP64 iterative refinement.
 cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
                         int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
-                        EcgGmresResult* out, cudaStream_t s);
+                        int reorth, EcgGmresResult* out, cudaStream_t s);
 // r = A x - b: infinity norm, rhs infinity norm (max(|b|inf, 1)) and nonfinite flag.
 cudaError_t pressure_residual(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x,
                               double* res_linf, double* rhs_norm, int* nonfinite, cudaStream_t s);

@@ -20,6 +20,11 @@ namespace ECG_NS {
 
 namespace imexk {
 
+// Cell indices r = j * nx + i fit 32 bits in every kernel here: the step
+// allocates the GMRES workspace, which rejects n >= 2^31 - 2^24 rows, before
+// it launches any of them.  Cell coordinates therefore come from a 32-bit
+// unsigned division.
+
 constexpr double kInf = __builtin_huge_val();
 constexpr double kLowest = -1.7976931348623157e308;
 constexpr double kMax = 1.7976931348623157e308;
@@ -277,7 +282,7 @@ __global__ void __launch_bounds__(NT) imex_star_kernel(const EcgFvParams P, cons
   long long mis_nf = 0;
   for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
        r += static_cast<long long>(gridDim.x) * NT) {
-    const int i = static_cast<int>(r % nx), j = static_cast<int>(r / nx);
+    const int j = static_cast<int>(static_cast<unsigned>(r) / static_cast<unsigned>(nx)), i = static_cast<int>(r) - j * nx;
     const Cons c = old_cell(P, u, i, j);
     const Cons w = old_cell(P, u, i - 1, j), e = old_cell(P, u, i + 1, j);
     const Cons s_ = old_cell(P, u, i, j - 1), nn = old_cell(P, u, i, j + 1);
@@ -317,7 +322,9 @@ __global__ void __launch_bounds__(NT) imex_star_kernel(const EcgFvParams P, cons
 // ---- faces ------------------------------------------------------------------------
 
 // Face enthalpies h_hat (mode 0) or energy fluxes h_hat * m_hat (mode 1) of
-// every x-face (nx+1 per row) and y-face (ny+1 per column).
+// every x-face (nx+1 per row) and y-face (ny+1 per column).  Thread c of row
+// j takes x-face (c, j) and y-face (c, j), which share the cell (c, j); rows
+// stride over grid.y, so no face index is divided.
 template <int NT>
 __global__ void __launch_bounds__(NT) imex_face_kernel(const EcgImexMap m, const double* __restrict__ S,
                                                        const double* __restrict__ p, const double* __restrict__ K,
@@ -325,19 +332,18 @@ __global__ void __launch_bounds__(NT) imex_face_kernel(const EcgImexMap m, const
                                                        unsigned char* __restrict__ fxf, unsigned char* __restrict__ fyf,
                                                        const int mode)
 {
-  const long long nfx = static_cast<long long>(m.nx + 1) * m.ny;
-  const long long nfy = static_cast<long long>(m.nx) * (m.ny + 1);
-  for (long long f = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; f < nfx + nfy;
-       f += static_cast<long long>(gridDim.x) * NT) {
-    if (f < nfx) {
-      const int fi = static_cast<int>(f % (m.nx + 1)), j = static_cast<int>(f / (m.nx + 1));
-      const FaceOut o = face_detail(m, S, p, K, fi - 1, j, fi, j, 0);
+  const int c = blockIdx.x * NT + threadIdx.x;
+  if (c > m.nx) return;
+  for (int j = blockIdx.y; j <= m.ny; j += gridDim.y) {
+    if (j < m.ny) {
+      const long long f = static_cast<long long>(j) * (m.nx + 1) + c;
+      const FaceOut o = face_detail(m, S, p, K, c - 1, j, c, j, 0);
       fxv[f] = mode ? o.flux : o.h_hat;
       if (fxf) fxf[f] = static_cast<unsigned char>(o.flags);
-    } else {
-      const long long g = f - nfx;
-      const int i = static_cast<int>(g % m.nx), fj = static_cast<int>(g / m.nx);
-      const FaceOut o = face_detail(m, S, p, K, i, fj - 1, i, fj, 1);
+    }
+    if (c < m.nx) {
+      const long long g = static_cast<long long>(j) * m.nx + c;
+      const FaceOut o = face_detail(m, S, p, K, c, j - 1, c, j, 1);
       fyv[g] = mode ? o.flux : o.h_hat;
       if (fyf) fyf[g] = static_cast<unsigned char>(o.flags);
     }
@@ -693,7 +699,7 @@ __global__ void __launch_bounds__(NT) imex_momentum_kernel(const EcgImexMap m, c
   long long nf = 0;
   for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
        r += static_cast<long long>(gridDim.x) * NT) {
-    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+    const int j = static_cast<int>(static_cast<unsigned>(r) / static_cast<unsigned>(m.nx)), i = static_cast<int>(r) - j * m.nx;
     const double gx = 0.5 * (p_b(m, p, i + 1, j) - p_b(m, p, i - 1, j)) * idx;
     const double gy = 0.5 * (p_b(m, p, i, j + 1) - p_b(m, p, i, j - 1)) * idy;
     const double k0 = S[r + n] - dt * gx, k1 = S[r + 2 * n] - dt * gy;
@@ -730,7 +736,7 @@ __global__ void __launch_bounds__(NT) imex_closeout_kernel(const EcgImexMap m, c
   double rsum = 0.0, msum = 0.0, esum = 0.0;
   for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
        r += static_cast<long long>(gridDim.x) * NT) {
-    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+    const int j = static_cast<int>(static_cast<unsigned>(r) / static_cast<unsigned>(m.nx)), i = static_cast<int>(r) - j * m.nx;
     const long long xe = static_cast<long long>(j) * (m.nx + 1) + i + 1, xw = xe - 1;
     const long long yn = static_cast<long long>(j + 1) * m.nx + i, ys = static_cast<long long>(j) * m.nx + i;
     const double fe = fx[xe], fw = fx[xw], fn = fy[yn], fs = fy[ys];
@@ -840,7 +846,7 @@ __global__ void __launch_bounds__(NT) imex_eq78_kernel(const EcgImexMap m, const
   };
   for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
        r += static_cast<long long>(gridDim.x) * NT) {
-    const int i = static_cast<int>(r % m.nx), j = static_cast<int>(r / m.nx);
+    const int j = static_cast<int>(static_cast<unsigned>(r) / static_cast<unsigned>(m.nx)), i = static_cast<int>(r) - j * m.nx;
     const double ue = vel(i + 1, j, 0), uw = vel(i - 1, j, 0), vn = vel(i, j + 1, 1), vs = vel(i, j - 1, 1);
     const double dv = 0.5 * (ue - uw) * idx + 0.5 * (vn - vs) * idy;
     // std::max({...}) keeps the first of equal maxima and skips NaN only in
@@ -922,8 +928,8 @@ inline cudaError_t imex_star(const EcgFvParams& P, const double* u, double dt, d
 inline cudaError_t imex_faces(const EcgImexMap& m, const double* S, const double* p, const double* K, double* fx,
                               double* fy, unsigned char* fxf, unsigned char* fyf, int mode, cudaStream_t s)
 {
-  const long long n = static_cast<long long>(m.nx + 1) * m.ny + static_cast<long long>(m.nx) * (m.ny + 1);
-  imexk::imex_face_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, p, K, fx, fy, fxf, fyf, mode);
+  const dim3 grid((m.nx + 256) / 256, m.ny + 1 < 65535 ? m.ny + 1 : 65535);
+  imexk::imex_face_kernel<256><<<grid, 256, 0, s>>>(m, S, p, K, fx, fy, fxf, fyf, mode);
   return cudaGetLastError();
 }
 

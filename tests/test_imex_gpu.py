@@ -62,12 +62,15 @@ def test_imex_step_fp64(gpu, name, arith):
     assert d.positivity_failure_count == int(c["d_positivity_failure_count"])
 
 
+@pytest.mark.parametrize("reorth", [0, 1])
 @pytest.mark.parametrize("name", golden_io.IMEX_NAMES)
-def test_imex_step_mixed_precision(gpu, name):
+def test_imex_step_mixed_precision(gpu, name, reorth):
     """FP32 inner GMRES + FP64 refinement: same FP64 stopping rule, so the
-    state agrees with the reference within the same 1e-9."""
+    state agrees with the reference within the same 1e-9, with the DGKS
+    second pass of the FP32 cycles on (1) or kept for severe cancellation
+    only (0, the default)."""
     c = golden_io.imex_case(name)
-    cfg, u1, d = _run(c, imex_precision="mixed")
+    cfg, u1, d = _run(c, imex_precision="mixed", mixed_reorth=reorth)
     assert d.solver_status in (1, 2), api.solver_status_str(d.solver_status)
     assert d.gmres_refinements >= 1
     assert golden_io.state_rel_err(u1, c["u1"]) <= 1e-9
