@@ -46,10 +46,8 @@ constexpr int kResidualBlocks = 148 * 2;  // grid of residual_kernel
 constexpr double kEps = 2.220446049250313e-16;
 
 struct GridBar {
-  unsigned int arrive;
-  unsigned int gen;
-  int timeout;
-  int pad;
+  unsigned int arrive;  // arrivals; the top bit is the timeout flag
+  unsigned int pad[3];
 };
 
 struct GmresArgs {
@@ -78,37 +76,51 @@ struct GmresArgs {
   long long spin_limit;
 };
 
-__device__ __forceinline__ unsigned int ld_volatile(const unsigned int* p) { return *reinterpret_cast<const volatile unsigned int*>(p); }
-__device__ __forceinline__ int ld_volatile_i(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
-
 // Grid-wide barrier over co-resident blocks (cooperative launch): one
 // arrival counter that only grows (zeroed by the host before the launch), so
-// barrier number g is passed once it reaches (g + 1) x blocks; one atomic per
-// block and no reset on the critical path.  The spin is bounded: a block that
-// waits longer than spin_limit polls sets the timeout flag and leaves; every
-// block then exits at its next check.
+// barrier number g is passed once it reaches (g + 1) x blocks; one release
+// atomic per block and no reset on the critical path.  The counter's top bit
+// is the timeout flag: a block that waits longer than spin_limit polls sets
+// it and leaves, every block polling sees it in the value it reads, and the
+// flag costs no load of its own after the barrier.
+constexpr unsigned int kBarTimeout = 0x80000000u;
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p)
+{
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned int atom_add_release(unsigned int* p, unsigned int x)
+{
+  unsigned int v;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "r"(x) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ bool grid_sync(GridBar* bar, unsigned int& gen, long long spin_limit)
 {
+  __shared__ int passed;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned int target = (gen + 1u) * gridDim.x;
-    __threadfence();
-    const unsigned int t = atomicAdd(&bar->arrive, 1u) + 1u;
-    if (t != target) {
-      long long spins = 0;
-      while (static_cast<int>(ld_volatile(&bar->arrive) - target) < 0) {
-        if (++spins > spin_limit) {
-          atomicExch(&bar->timeout, 1);
-          break;
-        }
-        __nanosleep(32);
+    unsigned int v = atom_add_release(&bar->arrive, 1u) + 1u;
+    long long spins = 0;
+    while (!(v & kBarTimeout) && static_cast<int>(v - target) < 0) {
+      if (++spins > spin_limit) {
+        atomicOr(&bar->arrive, kBarTimeout);
+        v |= kBarTimeout;
+        break;
       }
+      __nanosleep(32);
+      v = ld_acquire(&bar->arrive);
     }
-    __threadfence();
+    passed = (v & kBarTimeout) ? 0 : 1;
   }
   ++gen;
   __syncthreads();
-  return ld_volatile_i(&bar->timeout) == 0;
+  return passed != 0;
 }
 
 // source_map_index: wrap or even reflection (imex_source_map_helpers.hpp:169-188),
@@ -287,36 +299,60 @@ __device__ __forceinline__ void commit_partial(const double* wpart, double* dst)
   __syncthreads();
 }
 
-// out[q] = sum over blocks of part[b][q] (q < cnt), blocks in fixed groups,
-// groups in order: every block computes identical values.
-__device__ __forceinline__ void grid_reduce_redundant(const double* part, int ld, int cnt, double* out, double* scratch)
+__device__ __forceinline__ double nanmax(double m, double v) { return (m < v || v != v) ? v : m; }
+
+// out[q] for q < nsum + nmax, over the blocks' partial rows: the sum of
+// part[b][q] for q < nsum, the max (NaN propagates) for the nmax entries
+// after them.  Blocks go in fixed groups, each summed in block order by one
+// thread, and the groups in order: every block computes identical values.
+// Threads of a group read consecutive entries of one partial row; every load
+// of a batch is issued before the first add (indices clamped in range, the
+// surplus masked off), so a batch costs one L2 round trip.  Callers enter
+// right after a grid barrier, so no thread still reads out or scratch.
+__device__ __forceinline__ void grid_reduce_redundant(const double* part, int ld, int nsum, int nmax, double* out,
+                                                      double* scratch)
 {
+  constexpr int B = 16;  // loads in flight per thread
+  const int ne = nsum + nmax;
   const int nb = gridDim.x;
-  int groups = NT / cnt;
+  int groups = NT / ne;
   if (groups < 1) groups = 1;
+  if (groups > B) groups = B;
   const int per = (nb + groups - 1) / groups;
-  for (int t = threadIdx.x; t < cnt * groups; t += NT) {
-    const int q = t % cnt, gi = t / cnt;
+  for (int t = threadIdx.x; t < ne * groups; t += NT) {
+    const int q = t % ne, gi = t / ne;
+    const bool mx = q >= nsum;
     const int b0 = gi * per, b1 = b0 + per < nb ? b0 + per : nb;
     double s = 0.0;
-    for (int c0 = b0; c0 < b1; c0 += 16) {  // 16 loads in flight, summed in block order
-      double t[16];
+    for (int c0 = b0; c0 < b1; c0 += B) {
+      double v[B];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) t[k] = c0 + k < b1 ? __ldcg(part + static_cast<long long>(c0 + k) * ld + q) : 0.0;
+      for (int k = 0; k < B; ++k) v[k] = __ldcg(part + static_cast<long long>(c0 + k < b1 ? c0 + k : b1 - 1) * ld + q);
 #pragma unroll
-      for (int k = 0; k < 16; ++k)
-        if (c0 + k < b1) s += t[k];
+      for (int k = 0; k < B; ++k) {
+        const double r = mx ? nanmax(s, v[k]) : s + v[k];
+        s = c0 + k < b1 ? r : s;
+      }
     }
-    if (cnt * groups <= NT) scratch[gi * cnt + q] = s;
-    else scratch[q] = s;  // cnt > NT: one group
+    if (ne * groups <= NT) scratch[gi * ne + q] = s;
+    else scratch[q] = s;  // ne > NT: one group
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < cnt; q += NT) {
+  for (int q = threadIdx.x; q < ne; q += NT) {
+    const bool mx = q >= nsum;
     double s = 0.0;
-    if (cnt * groups <= NT)
-      for (int gi = 0; gi < groups; ++gi) s += scratch[gi * cnt + q];
-    else
+    if (ne * groups <= NT) {
+      double v[B];
+#pragma unroll
+      for (int gi = 0; gi < B; ++gi) v[gi] = scratch[(gi < groups ? gi : groups - 1) * ne + q];
+#pragma unroll
+      for (int gi = 0; gi < B; ++gi) {
+        const double r = mx ? nanmax(s, v[gi]) : s + v[gi];
+        s = gi < groups ? r : s;
+      }
+    } else {
       s = scratch[q];
+    }
     out[q] = s;
   }
   __syncthreads();
@@ -332,8 +368,6 @@ __device__ __forceinline__ double sum_squares(const double* red, int k)
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   return s;
 }
-
-__device__ __forceinline__ double nanmax(double m, double v) { return (m < v || v != v) ? v : m; }
 
 __device__ __forceinline__ double warp_max(double m)
 {
@@ -354,20 +388,6 @@ __device__ __forceinline__ void block_max_partial(double v, double* part_row, in
     part_row[q] = m;
   }
   __syncthreads();
-}
-
-__device__ __forceinline__ double grid_max_redundant(const double* part, int ld, int q, double* scratch)
-{
-  double m = 0.0;
-  for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += NT)
-    m = nanmax(m, __ldcg(part + static_cast<long long>(b) * ld + q));
-  m = warp_max(m);
-  if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = m;
-  __syncthreads();
-  double r = scratch[0];
-  for (int w = 1; w < NW; ++w) r = nanmax(r, scratch[w]);
-  __syncthreads();
-  return r;
 }
 
 struct SolveState {
@@ -621,11 +641,9 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
                              double* shbase)
 {
   const long long n = a.n;
-  const int nx = a.op.nx;
   const Rows rw = own_rows(n);
   const bool wide = rw.r1 - rw.r0 > NT;  // two rows a thread per pass
   const int ld = a.ld;
-  const int XSLOT = ld - 1;  // block max of |r_j|, read after the next barrier
   double* part_row = a.part + static_cast<long long>(blockIdx.x) * ld;
   const Smem S = carve(shbase, a.m);
   SolveState st;
@@ -637,24 +655,24 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   st.converged = st.breakdown = st.nonfinite = st.timeout = st.restart = 0;
   double beta = 0.0;
 
-  // ---- r0 = b - A x0: ||b||inf, ||r0||inf, ||r0||2 ----
+  // ---- r0 = b - A x0: ||r0||2, ||b||inf, ||r0||inf ----
   {
     double bmax = 0.0, rmax = 0.0, r2 = 0.0;
     if (wide) sweep_r0<2>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
     else sweep_r0<1>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
-    block_max_partial(bmax, part_row, 0, S.scratch);
-    block_max_partial(rmax, part_row, 1, S.scratch);
     warp_partial(r2, S.wpart);
-    commit_partial(S.wpart, part_row + 2);
+    commit_partial(S.wpart, part_row);
+    block_max_partial(bmax, part_row, 1, S.scratch);
+    block_max_partial(rmax, part_row, 2, S.scratch);
   }
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
     st.timeout = 1;
     return st;
   }
-  const double bn_raw = grid_max_redundant(a.part, ld, 0, S.scratch);
-  const double r0inf = grid_max_redundant(a.part, ld, 1, S.scratch);
-  grid_reduce_redundant(a.part + 2, ld, 1, S.red, S.scratch);
+  grid_reduce_redundant(a.part, ld, 1, 2, S.red, S.scratch);
   beta = sqrt(S.red[0]);
+  const double bn_raw = S.red[1];
+  const double r0inf = S.red[2];
   st.r0_linf = r0inf;
   st.b_linf = bn_raw;
   const double bn = bn_raw > 1.0 ? bn_raw : 1.0;
@@ -686,40 +704,45 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     __syncthreads();
   }
   bool broke = false;
+  // update_best / convergence test of iterate j (residual r_{j-1}, whose
+  // block maxima sweep C of iteration j-1 left in slot j+3); true: stop
+  auto check = [&](int j, double linf) {
+    if (!isfinite(linf)) {
+      st.nonfinite = 1;
+      return true;
+    }
+    if (linf < st.best_linf) {
+      st.best_linf = linf;
+      st.best_it = j;
+    }
+    if (linf <= tol || linf / bn <= tol) {
+      st.converged = 1;
+      st.best_it = j;
+      st.best_linf = linf;
+      return true;
+    }
+    if (linf <= rtarget) {
+      st.restart = 1;
+      st.best_it = j;
+      st.best_linf = linf;
+      return true;
+    }
+    return false;
+  };
   for (int j = 0; !stop; ++j) {
     if (!grid_sync(a.bar, gen, a.spin_limit)) {
       st.timeout = 1;
       return st;
     }
-    if (j > 0) {
-      // update_best / convergence test of iterate j (residual r_{j-1})
-      const double linf = grid_max_redundant(a.part, ld, XSLOT, S.scratch);
-      if (!isfinite(linf)) {
-        st.nonfinite = 1;
-        break;
+    if (broke || j >= kmax) {
+      // no further column: the test of iterate j on its own
+      if (j > 0) {
+        grid_reduce_redundant(a.part + j + 3, ld, 0, 1, S.red, S.scratch);
+        if (check(j, S.red[0])) break;
       }
-      if (linf < st.best_linf) {
-        st.best_linf = linf;
-        st.best_it = j;
-      }
-      if (linf <= tol || linf / bn <= tol) {
-        st.converged = 1;
-        st.best_it = j;
-        st.best_linf = linf;
-        break;
-      }
-      if (linf <= rtarget) {
-        st.restart = 1;
-        st.best_it = j;
-        st.best_linf = linf;
-        break;
-      }
-    }
-    if (broke) {
-      st.breakdown = 1;
+      if (broke) st.breakdown = 1;
       break;
     }
-    if (j >= kmax) break;
     const TV* vj = V + static_cast<long long>(j) * n;
     // ---- sweep A: w = A v_j; d_i = v_i . w (i <= j); ||w||^2; nonfinite ----
     if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
@@ -729,7 +752,11 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       st.timeout = 1;
       return st;
     }
-    grid_reduce_redundant(a.part, ld, j + 3, S.red, S.scratch);
+    // the dot products and, in the same pass, the residual maxima of iterate
+    // j: the test runs here, one sweep A later than its data, so it costs no
+    // pass of its own (a stopping iterate discards this w)
+    grid_reduce_redundant(a.part, ld, j + 3, j > 0 ? 1 : 0, S.red, S.scratch);
+    if (j > 0 && check(j, S.red[j + 3])) break;
     if (S.red[j + 2] != 0.0) {
       st.nonfinite = 1;
       break;
@@ -756,7 +783,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
         st.timeout = 1;
         return st;
       }
-      grid_reduce_redundant(a.part, ld, j + 2, S.red, S.scratch);
+      grid_reduce_redundant(a.part, ld, j + 2, 0, S.red, S.scratch);
       sw = S.red[j + 1];
       nn2 = sw - sum_squares(S.red, j + 1);
       for (int q = threadIdx.x; q <= j; q += NT) {
@@ -818,7 +845,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     const double rmx = wide ? sweep_next<TV, 2>(rw, V, n, S.coef, j + 1, w, vn, inv_nn, cr1, cr2, rres)
                             : sweep_next<TV, 1>(rw, V, n, S.coef, j + 1, w, vn, inv_nn, cr1, cr2, rres);
     st.it = j + 1;
-    block_max_partial(rmx, part_row, XSLOT, S.scratch);
+    block_max_partial(rmx, part_row, j + 4, S.scratch);  // slot (j+1)+3, read after the next sweep A
   }
   // ---- x = x0 + V_k y_k for the returned iterate k ----
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
@@ -917,8 +944,9 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
     block_max_partial(bmax, part_row, 1, S.scratch);
     if (grid_sync(a.bar, gen, a.spin_limit)) {
       if (blockIdx.x == 0) {
-        out.final_linf = grid_max_redundant(a.part, a.ld, 0, S.scratch);
-        out.final_b_linf = grid_max_redundant(a.part, a.ld, 1, S.scratch);
+        grid_reduce_redundant(a.part, a.ld, 0, 2, S.red, S.scratch);
+        out.final_linf = S.red[0];
+        out.final_b_linf = S.red[1];
       }
     } else {
       out.timeout = 1;
