@@ -73,6 +73,8 @@ struct GmresArgs {
   double inner_rtol;  // mixed: restart when the recurrence residual fell by this factor
   int max_refine;     // mixed: cycles
   int reorth;         // mixed: DGKS test of the FP32-basis cycles, 1 as the FP64 solve, 0 severe cancellation only
+  int kres;           // basis vectors resident in shared memory on each block's rows
+  int prow;           // rows of a block (the last may have fewer)
   long long spin_limit;
 };
 
@@ -148,16 +150,55 @@ __device__ __forceinline__ double ldv(const TV* p)
   return static_cast<double>(__ldcg(p));
 }
 
-// acc[r] + sgn sum_{i<cnt} c[i] V_i[q_r] for R rows at once, i ascending (the
-// rounding of the plain loop), with 32 (FP64) or 16 (FP32) loads of the basis in flight before
-// the first FMA (the stores that follow a call would otherwise keep the
-// compiler from starting the next row's loads: the new basis vector aliases V).
+// The Krylov basis: V in global memory ((m+1) x n, the copy other blocks'
+// operator rows read), and its first K vectors on the block's own rows
+// r0 .. r0+P-1 also resident in shared memory (vector i, row q at
+// s[i P + q - r0]), where the block's dot products and combinations read
+// them without an L2 round trip.
+template <typename TV>
+struct Basis {
+  TV* V;
+  long long n;
+  TV* s;
+  int K, P, r0;
+  __device__ __forceinline__ TV* vec(int i) const { return V + static_cast<long long>(i) * n; }
+  __device__ __forceinline__ void store(int i, int q, TV v) const
+  {
+    V[static_cast<long long>(i) * n + q] = v;
+    if (i < K) s[i * P + q - r0] = v;
+  }
+};
+
+// acc[r] + sgn sum_{i<cnt} c[i] V_i[q_r] for R rows q_r of the block at once,
+// i ascending (the rounding of the plain loop): the resident vectors from
+// shared memory, then the rest with 32 (FP64) or 16 (FP32) loads in flight
+// before the first FMA (the stores that follow a call would otherwise keep
+// the compiler from starting the next row's loads: the new basis vector
+// aliases V).
 template <typename TV, bool SUB, int R>
-__device__ __forceinline__ void basis_combine(double (&acc)[R], const TV* __restrict__ V, long long n, const int (&q)[R],
-                                              const double* c, int cnt)
+__device__ __forceinline__ void basis_combine(double (&acc)[R], const Basis<TV>& bs, const int (&q)[R], const double* c,
+                                              int cnt)
 {
   constexpr int B = (sizeof(TV) == 8 ? 32 : 16) / R;
-  for (int i0 = 0; i0 < cnt; i0 += B) {
+  const int ks = cnt < bs.K ? cnt : bs.K;
+  for (int i0 = 0; i0 < ks; i0 += B) {
+    TV a[R][B];
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+#pragma unroll
+      for (int r = 0; r < R; ++r) a[r][k] = bs.s[(i0 + k < ks ? i0 + k : ks - 1) * bs.P + q[r] - bs.r0];
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+      if (i0 + k < ks) {
+        const double ck = c[i0 + k];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          acc[r] = SUB ? acc[r] - ck * static_cast<double>(a[r][k]) : acc[r] + ck * static_cast<double>(a[r][k]);
+      }
+  }
+  const TV* __restrict__ V = bs.V;
+  const long long n = bs.n;
+  for (int i0 = ks; i0 < cnt; i0 += B) {
     TV a[R][B];
 #pragma unroll
     for (int k = 0; k < B; ++k)
@@ -257,6 +298,7 @@ struct Smem {
   double* coef;
   double* wpart;
   double* scratch;
+  double* vs;  // resident basis vectors (TV)
   double* dpart;
 };
 __device__ __forceinline__ Smem carve(double* base, int m)
@@ -272,8 +314,10 @@ __device__ __forceinline__ Smem carve(double* base, int m)
   s.wpart = s.coef + L;
   s.scratch = s.wpart + NW;
   s.dpart = s.scratch + NT + L;
+  s.vs = s.dpart + NW * dots_ld(m);
   return s;
 }
+// bytes of the fixed part; the resident basis vectors follow it
 inline size_t smem_bytes(int m)
 {
   return sizeof(double) * (static_cast<size_t>(7) * (m + 8) + NW + NT + static_cast<size_t>(NW) * dots_ld(m));
@@ -445,9 +489,11 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&s)[DG], int lane)
 // (w read once a pass), a reduce-scatter of the DG sums in each warp, then
 // the warps' partials summed in warp order.
 template <typename TV>
-__device__ __forceinline__ void block_dots(const TV* __restrict__ V, long long n, const double* __restrict__ w, Rows rw,
-                                           int nvec, bool with_norm, double* part_row, double* dpart)
+__device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __restrict__ w, Rows rw, int nvec,
+                                           bool with_norm, double* part_row, double* dpart)
 {
+  const TV* __restrict__ V = bs.V;
+  const long long n = bs.n;
   constexpr int DG = DG_ROWS;
   constexpr int SMALL = 16;  // rows a lane holds in the small-block layout
   __syncthreads();  // w of the block's rows is complete
@@ -466,10 +512,16 @@ __device__ __forceinline__ void block_dots(const TV* __restrict__ V, long long n
     for (int i = warp; i < tot; i += NW) {
       double sm = 0.0;
       if (i < nvec) {
-        const TV* pv = V + static_cast<long long>(i) * n + rw.r0 + lane;  // rows at immediate offsets
         TV av[SMALL];
+        if (i < bs.K) {
+          const TV* pv = bs.s + i * bs.P + lane;
 #pragma unroll
-        for (int k = 0; k < SMALL; ++k) av[k] = rw.r0 + lane + 32 * k < rw.r1 ? __ldcg(pv + 32 * k) : TV(0);
+          for (int k = 0; k < SMALL; ++k) av[k] = rw.r0 + lane + 32 * k < rw.r1 ? pv[32 * k] : TV(0);
+        } else {
+          const TV* pv = V + static_cast<long long>(i) * n + rw.r0 + lane;  // rows at immediate offsets
+#pragma unroll
+          for (int k = 0; k < SMALL; ++k) av[k] = rw.r0 + lane + 32 * k < rw.r1 ? __ldcg(pv + 32 * k) : TV(0);
+        }
 #pragma unroll
         for (int k = 0; k < SMALL; ++k) sm += static_cast<double>(av[k]) * wr[k];
       } else if (i == nvec) {
@@ -498,10 +550,18 @@ __device__ __forceinline__ void block_dots(const TV* __restrict__ V, long long n
       const int qb = hb ? q + NT : q;
       const double wq[2] = {w[q], hb ? w[qb] : 0.0};
       TV a[2][DG];
+      if (g0 + DG <= bs.K) {  // a group of resident vectors
 #pragma unroll
-      for (int k = 0; k < DG; ++k) {
-        a[0][k] = g0 + k < nvec ? __ldcg(V + static_cast<long long>(g0 + k) * n + q) : TV(0);
-        a[1][k] = g0 + k < nvec && hb ? __ldcg(V + static_cast<long long>(g0 + k) * n + qb) : TV(0);
+        for (int k = 0; k < DG; ++k) {
+          a[0][k] = bs.s[(g0 + k) * bs.P + q - rw.r0];
+          a[1][k] = hb ? bs.s[(g0 + k) * bs.P + qb - rw.r0] : TV(0);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < DG; ++k) {
+          a[0][k] = g0 + k < nvec ? __ldcg(V + static_cast<long long>(g0 + k) * n + q) : TV(0);
+          a[1][k] = g0 + k < nvec && hb ? __ldcg(V + static_cast<long long>(g0 + k) * n + qb) : TV(0);
+        }
       }
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
@@ -575,8 +635,8 @@ __device__ __forceinline__ void sweep_spmv(const EcgPressureOp& op, Rows rw, con
 
 // out = in + sgn V c (cnt basis vectors) on the block's rows.
 template <typename TV, bool SUB, int R>
-__device__ __forceinline__ void sweep_combine(Rows rw, const TV* __restrict__ V, long long n, const double* c, int cnt,
-                                              const double* in, double* out)
+__device__ __forceinline__ void sweep_combine(Rows rw, const Basis<TV>& bs, const double* c, int cnt, const double* in,
+                                              double* out)
 {
   for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += R * NT) {
     int qq[R];
@@ -586,18 +646,18 @@ __device__ __forceinline__ void sweep_combine(Rows rw, const TV* __restrict__ V,
       qq[r] = q + r * NT < rw.r1 ? q + r * NT : q;
       acc[r] = in[qq[r]];
     }
-    basis_combine<TV, SUB, R>(acc, V, n, qq, c, cnt);
+    basis_combine<TV, SUB, R>(acc, bs, qq, c, cnt);
 #pragma unroll
     for (int r = 0; r < R; ++r)
       if (q + r * NT < rw.r1) out[qq[r]] = acc[r];
   }
 }
 
-// w - V c -> v_{j+1} = (w - V c) inv_nn (stored as TV), and the residual
-// recurrence rres <- cr1 rres + cr2 v_{j+1}; returns the block-local max |rres|.
+// w - V c -> v_cnt = (w - V c) inv_nn (stored as TV), and the residual
+// recurrence rres <- cr1 rres + cr2 v_cnt; returns the block-local max |rres|.
 template <typename TV, int R>
-__device__ __forceinline__ double sweep_next(Rows rw, const TV* __restrict__ V, long long n, const double* c, int cnt,
-                                             const double* __restrict__ w, TV* vn, double inv_nn, double cr1, double cr2,
+__device__ __forceinline__ double sweep_next(Rows rw, const Basis<TV>& bs, const double* c, int cnt,
+                                             const double* __restrict__ w, double inv_nn, double cr1, double cr2,
                                              double* __restrict__ rres)
 {
   double rmx = 0.0;
@@ -610,12 +670,12 @@ __device__ __forceinline__ double sweep_next(Rows rw, const TV* __restrict__ V, 
       acc[r] = w[qq[r]];
       rp[r] = rres[qq[r]];
     }
-    basis_combine<TV, true, R>(acc, V, n, qq, c, cnt);
+    basis_combine<TV, true, R>(acc, bs, qq, c, cnt);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if (q + r * NT >= rw.r1) break;
       const TV vq = static_cast<TV>(acc[r] * inv_nn);
-      vn[qq[r]] = vq;
+      bs.store(cnt, qq[r], vq);
       const double rq = cr1 * rp[r] + cr2 * static_cast<double>(vq);
       rres[qq[r]] = rq;
       rmx = nanmax(rmx, fabs(rq));
@@ -634,7 +694,7 @@ __device__ __forceinline__ double sweep_next(Rows rw, const TV* __restrict__ V, 
 // restart_rtol ||r_0||inf.  x0vec and xvec may be the same array (a restart):
 // each row of x is read and then written by one thread, after the last read
 // of x0 by any other row.
-template <typename TV>
+template <typename TV, bool RES>
 __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec, const double* x0vec, double* xvec,
                              TV* __restrict__ V, double* __restrict__ w,
                              double* __restrict__ rres, int kmax, double tol, double restart_rtol, unsigned int& gen,
@@ -646,6 +706,9 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   const int ld = a.ld;
   double* part_row = a.part + static_cast<long long>(blockIdx.x) * ld;
   const Smem S = carve(shbase, a.m);
+  // RES = false: no resident vectors (K a constant 0, the shared-memory
+  // paths compiled out, the register budget of the plain solve)
+  const Basis<TV> bs{V, n, reinterpret_cast<TV*>(S.vs), RES ? a.kres : 0, a.prow, rw.r0};
   SolveState st;
   st.it = 0;
   st.best_it = 0;
@@ -699,7 +762,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   }
   const double btol = kEps * 100.0 * (beta > 1.0 ? beta : 1.0);
   if (!stop) {
-    for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) V[q] = static_cast<TV>(w[q] / beta);
+    for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) bs.store(0, q, static_cast<TV>(w[q] / beta));
     if (threadIdx.x == 0) S.g[0] = beta;
     __syncthreads();
   }
@@ -747,7 +810,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     // ---- sweep A: w = A v_j; d_i = v_i . w (i <= j); ||w||^2; nonfinite ----
     if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
     else sweep_spmv<TV, 1>(a.op, rw, vj, w);
-    block_dots<TV>(V, n, w, rw, j + 1, true, part_row, S.dpart);
+    block_dots<TV>(bs, w, rw, j + 1, true, part_row, S.dpart);
     if (!grid_sync(a.bar, gen, a.spin_limit)) {
       st.timeout = 1;
       return st;
@@ -776,9 +839,9 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     const double eta = (sizeof(TV) == 8 || a.reorth) ? 0.5 : 1.0e-6;
     if (!(nn2 >= eta * sw)) {
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
-      if (wide) sweep_combine<TV, true, 2>(rw, V, n, S.coef, j + 1, w, w);
-      else sweep_combine<TV, true, 1>(rw, V, n, S.coef, j + 1, w, w);
-      block_dots<TV>(V, n, w, rw, j + 1, true, part_row, S.dpart);
+      if (wide) sweep_combine<TV, true, 2>(rw, bs, S.coef, j + 1, w, w);
+      else sweep_combine<TV, true, 1>(rw, bs, S.coef, j + 1, w, w);
+      block_dots<TV>(bs, w, rw, j + 1, true, part_row, S.dpart);
       if (!grid_sync(a.bar, gen, a.spin_limit)) {
         st.timeout = 1;
         return st;
@@ -839,11 +902,10 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     }
     broke = !(nn > btol);
     // ---- sweep C: w <- w - V coef; v_{j+1} = w / nn; r_j recurrence ----
-    TV* vn = V + static_cast<long long>(j + 1) * n;
     const double inv_nn = broke ? 0.0 : 1.0 / nn;
     const double cr1 = s * s, cr2 = -s * c * gam;
-    const double rmx = wide ? sweep_next<TV, 2>(rw, V, n, S.coef, j + 1, w, vn, inv_nn, cr1, cr2, rres)
-                            : sweep_next<TV, 1>(rw, V, n, S.coef, j + 1, w, vn, inv_nn, cr1, cr2, rres);
+    const double rmx = wide ? sweep_next<TV, 2>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres)
+                            : sweep_next<TV, 1>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
     st.it = j + 1;
     block_max_partial(rmx, part_row, j + 4, S.scratch);  // slot (j+1)+3, read after the next sweep A
   }
@@ -861,11 +923,12 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   for (int q = 0; q < k; ++q) ynf |= !isfinite(y[q]);
   if (ynf) st.nonfinite = 1;
   if (ynf) k = 0;  // x = x0
-  if (wide) sweep_combine<TV, false, 2>(rw, V, n, y, k, x0vec, xvec);
-  else sweep_combine<TV, false, 1>(rw, V, n, y, k, x0vec, xvec);
+  if (wide) sweep_combine<TV, false, 2>(rw, bs, y, k, x0vec, xvec);
+  else sweep_combine<TV, false, 1>(rw, bs, y, k, x0vec, xvec);
   return st;
 }
 
+template <bool RES>
 __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
 {
   extern __shared__ double sh[];
@@ -875,7 +938,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   const int limit = a.max_iter < a.n ? a.max_iter : static_cast<int>(a.n);
   if (!a.mixed) {
     const SolveState st =
-        krylov<double>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, sh);
+        krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, sh);
     out.iterations = st.best_it;
     out.converged = st.converged;
     out.breakdown = st.breakdown;
@@ -897,7 +960,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
       const int left = limit - total;
       const bool last = cycles + 1 >= a.max_refine;
       const int kin = per_cycle < left ? per_cycle : left;
-      st = krylov<float>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol, gen,
+      st = krylov<float, RES>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol, gen,
                          sh);
       if (cycles == 0) {
         out.initial_linf = st.r0_linf;
@@ -996,6 +1059,8 @@ struct EcgGmresWork {
   EcgGmresResult* h_res = nullptr;
   double* h_part = nullptr;
   size_t smem = 0;
+  int kres = 0;  // basis vectors resident in shared memory
+  int prow = 0;  // rows of a block
 };
 
 EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int device, bool mixed, std::string* err)
@@ -1011,12 +1076,34 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   if (w->m > n) w->m = static_cast<int>(n);
   w->device = device;
   w->mixed = mixed;
-  w->smem = smem_bytes(w->m);
   // one block per SM (every SM's share of bandwidth), fewer for tiny systems
   const long long want = (n + 63) / 64;
   const long long cap = num_sms;
   w->nblocks = static_cast<int>(want < cap ? (want < 1 ? 1 : want) : cap);
   w->ld = w->m + 8;
+  // The shared memory left over by the fixed part holds the first basis
+  // vectors on the block's rows (one block per SM, so the whole opt-in
+  // budget is the block's).
+  w->prow = static_cast<int>((n + w->nblocks - 1) / w->nblocks);
+  int optin = 0;
+  cudaFuncAttributes fa;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, gmres_kernel<true>) != cudaSuccess) {
+    if (err) *err = "gmres kernel attributes unavailable";
+    delete w;
+    return nullptr;
+  }
+  const size_t budget = static_cast<size_t>(optin) - fa.sharedSizeBytes;
+  const size_t fixed = smem_bytes(w->m);
+  const size_t vbytes = static_cast<size_t>(w->prow) * (mixed ? sizeof(float) : sizeof(double));
+  long long kres = budget > fixed ? static_cast<long long>((budget - fixed) / vbytes) : 0;
+  if (kres > w->m + 1) kres = w->m + 1;
+  // A few resident vectors save less than the L1 cache they displace costs
+  // the operator's loads (measured at 768^2: 5 FP64 / 11 FP32 vectors, 16-20 %
+  // slower), so residency needs 32 vectors or the whole basis.
+  if (kres < 32 && kres < w->m + 1) kres = 0;
+  w->kres = static_cast<int>(kres);
+  w->smem = fixed + static_cast<size_t>(kres) * vbytes;
   bool ok = true;
   auto alloc = [&](void** p, size_t bytes) {
     if (ok && cudaMalloc(p, bytes) != cudaSuccess) ok = false;
@@ -1035,11 +1122,16 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   if (ok && cudaMallocHost(&w->h_res, sizeof(EcgGmresResult)) != cudaSuccess) ok = false;
   if (ok && cudaMallocHost(&w->h_part, sizeof(double) * 2 * kResidualBlocks) != cudaSuccess) ok = false;
   if (ok && cudaMemset(w->bar, 0, sizeof(GridBar)) != cudaSuccess) ok = false;
-  if (ok && cudaFuncSetAttribute(gmres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(w->smem)) !=
-                cudaSuccess)
+  // the whole budget, so workspaces of any size can launch
+  if (ok && (cudaFuncSetAttribute(gmres_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(budget)) != cudaSuccess ||
+             cudaFuncSetAttribute(gmres_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(budget)) != cudaSuccess))
     ok = false;
   int per_sm = 0;
-  if (ok && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_kernel, NT, w->smem) != cudaSuccess || per_sm < 1)) {
+  if (ok && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, w->kres > 0 ? gmres_kernel<true> : gmres_kernel<false>,
+                                                           NT, w->smem) != cudaSuccess ||
+             per_sm < 1)) {
     if (err) *err = "gmres kernel does not fit on one SM with its shared memory";
     gmres_work_destroy(w);
     return nullptr;
@@ -1097,11 +1189,14 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.inner_rtol = inner_rtol;
   a.max_refine = max_refine;
   a.reorth = reorth;
+  a.kres = w->kres;
+  a.prow = w->prow;
   a.spin_limit = 1LL << 25;  // ~2 s of polling before a barrier gives up
   cudaError_t e = cudaMemsetAsync(w->bar, 0, sizeof(GridBar), s);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
-  e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(gmres_kernel), dim3(w->nblocks), dim3(NT), args, w->smem, s);
+  void* kern = w->kres > 0 ? reinterpret_cast<void*>(gmres_kernel<true>) : reinterpret_cast<void*>(gmres_kernel<false>);
+  e = cudaLaunchCooperativeKernel(kern, dim3(w->nblocks), dim3(NT), args, w->smem, s);
   if (e != cudaSuccess) return e;
   e = cudaMemcpyAsync(w->h_res, w->d_res, sizeof(EcgGmresResult), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return e;
