@@ -860,6 +860,27 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       st.nonfinite = 1;
       break;
     }
+    broke = !(nn > btol);
+    const double inv_nn = broke ? 0.0 : 1.0 / nn;
+    // ---- sweep C, first half, on few-row blocks (one row a thread of warps
+    // 1-15): w <- w - V coef, v_{j+1} = w / nn, while thread 0 rotates; the
+    // recurrence, which needs the rotation, follows from registers ----
+    const bool overlap = rw.r1 - rw.r0 <= NT - 32;
+    int qv = -1;
+    double vqd = 0.0, rp = 0.0;
+    if (overlap && threadIdx.x >= 32) {
+      const int q = rw.r0 + static_cast<int>(threadIdx.x) - 32;
+      if (q < rw.r1) {
+        const int qq[1] = {q};
+        double acc[1] = {w[q]};
+        rp = rres[q];
+        basis_combine<TV, true, 1>(acc, bs, qq, S.coef, j + 1);
+        const TV vq = static_cast<TV>(acc[0] * inv_nn);
+        bs.store(j + 1, q, vq);
+        vqd = static_cast<double>(vq);
+        qv = q;
+      }
+    }
     // ---- Givens rotation of the new column (identical in every block) ----
     if (threadIdx.x == 0) {
       // the running entry stays in a register; the rotations and the column
@@ -900,12 +921,19 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       st.nonfinite = 1;
       break;
     }
-    broke = !(nn > btol);
     // ---- sweep C: w <- w - V coef; v_{j+1} = w / nn; r_j recurrence ----
-    const double inv_nn = broke ? 0.0 : 1.0 / nn;
     const double cr1 = s * s, cr2 = -s * c * gam;
-    const double rmx = wide ? sweep_next<TV, 2>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres)
-                            : sweep_next<TV, 1>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
+    double rmx = 0.0;
+    if (overlap) {
+      if (qv >= 0) {
+        const double rq = cr1 * rp + cr2 * vqd;
+        rres[qv] = rq;
+        rmx = nanmax(rmx, fabs(rq));
+      }
+    } else {
+      rmx = wide ? sweep_next<TV, 2>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres)
+                 : sweep_next<TV, 1>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
+    }
     st.it = j + 1;
     block_max_partial(rmx, part_row, j + 4, S.scratch);  // slot (j+1)+3, read after the next sweep A
   }
