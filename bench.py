@@ -31,9 +31,10 @@ body compute_euler_dt -> euler_fv_one_step -> compute_diagnostics.
 
 Two more measurements ride on the same JSON line at N=1 (skip them with
 --no-extra-legs): "imex", the second half of the metric (Gresho vortex at
-M = 0.01 on 256^2 and on 768^2, IMEX T1/S2: ms per step of the all-FP64 GMRES
-solve and of the FP32-basis / FP64-arithmetic solve, their iterations, and
-the relative drift between the two states), and "batched" (64 seeded Riemann
+M = 0.01 on 256^2 and on 768^2, and the 2560x640 bubble, IMEX T1/S2: ms per
+step of the all-FP64 GMRES solve and of the FP32-basis / FP64-arithmetic
+solve, their iterations, and the relative drift between the two states; its
+mixed_speedup is the 256^2 Gresho case's), and "batched" (64 seeded Riemann
 solves of uneven sizes advanced by one persistent launch per step for 200
 steps).
 
@@ -280,26 +281,39 @@ def imex_kv(n, mach):
     }
 
 
-# (name, grid, Mach): the Gresho configuration of the metric, and a grid whose
+def bubble_imex_kv(nx, ny):
+    """The shock-density bubble's IMEX settings (imex_cfl 0.45, 4 Picard
+    passes, GMRES tol 1e-10 / 200 iterations, no acoustic start-up or cap)."""
+    return {
+        "amr.n_cell": f"{nx} {ny}", "geometry.prob_hi": "2 0.5", "euler.problem": "shock_density_bubble_2d",
+        "euler.method": "imex", "euler.spatial_order": 2, "euler.imex_acoustic_startup": 0,
+        "euler.imex_acoustic_cfl_cap": 0, "euler.imex_picard_iterations": 4, "euler.imex_solver_tol": "1e-10",
+        "euler.imex_solver_max_iter": 200, "euler.imex_cfl": 0.45, "stop_time": 1.0,
+    }
+
+
+# (name, configuration): the Gresho configuration of the metric, a grid whose
 # Krylov basis no longer fits in L2 (the FP32 basis halves the bytes of the
-# sweeps that dominate there; at 256^2 the solve is bound by barrier latency)
-IMEX_CASES = [("gresho_vortex 256x256 periodic, M=0.01", 256, 0.01),
-              ("gresho_vortex 768x768 periodic, M=0.01", 768, 0.01)]
+# sweeps that dominate there; at 256^2 the solve is bound by barrier latency),
+# and the bubble's IMEX step (a few GMRES iterations a solve)
+IMEX_CASES = [("gresho_vortex 256x256 periodic, M=0.01", imex_kv(256, 0.01)),
+              ("gresho_vortex 768x768 periodic, M=0.01", imex_kv(768, 0.01)),
+              ("shock_density_bubble_2d 2560x640", bubble_imex_kv(2560, 640))]
 
 
 def imex_leg(dev, stream, steps=3):
-    """Gresho vortex, IMEX T1/S2 (4 Picard solves, GMRES tol 1e-10): time per
-    step of the all-FP64 solve and of the FP32-basis / FP64-arithmetic solve
-    on the same GPU, their GMRES iterations, and the relative drift between
-    their states after `steps` + 1 steps."""
+    """Each IMEX_CASES configuration, IMEX T1/S2 (4 Picard solves, GMRES tol
+    1e-10): time per step of the all-FP64 solve and of the FP32-basis /
+    FP64-arithmetic solve on the same GPU, their GMRES iterations, and the
+    relative drift between their states after `steps` + 1 steps."""
     import torch
 
     from amrex_euler_allmach_explicit_imex_b200 import api
     from amrex_euler_allmach_explicit_imex_b200.config import read_config
 
     cases = []
-    for name, n, mach in IMEX_CASES:
-        cfg = read_config(imex_kv(n, mach)).cfg
+    for name, kv in IMEX_CASES:
+        cfg = read_config(kv).cfg
         out = {}
         states = {}
         for prec in ("fp64", "mixed"):
