@@ -1,5 +1,6 @@
 // GMRES pressure solve of the IMEX step: one persistent cooperative launch
-// per solve, matrix-free operator, deterministic grid reductions.
+// per solve, matrix-free operator, grid reductions through accumulator rows
+// that every block reads after a barrier.
 //
 // Reference semantics (solve_host_sparse_gmres, imex/imex_pressure_helpers.hpp:92-217):
 // unrestarted GMRES from x0 with iterations_limit = min(max_iter, n); the
@@ -60,7 +61,8 @@ struct GmresArgs {
   double* w;     // n
   double* r;     // n: residual recurrence
   float* V32;    // (m+1) x n (mixed)
-  double* part;  // nblocks x ld
+  double* part;  // residual_kernel: 2 x its blocks
+  double* acc;   // three accumulator rows of ld doubles, zeroed by the host before the launch
   double* R;     // column-major (m+1) x m
   GridBar* bar;
   EcgGmresResult* res;
@@ -331,76 +333,57 @@ __device__ __forceinline__ void warp_partial(double v, double* wpart)
   if ((threadIdx.x & 31) == 0) wpart[threadIdx.x >> 5] = v;
 }
 
-// *dst = sum of the warp partials in warp order.
-__device__ __forceinline__ void commit_partial(const double* wpart, double* dst)
+// Grid sums and maxima go through accumulator rows: every block adds its
+// partial sums (or raises its partial maxima) into entry q of one row, a grid
+// barrier follows, and every block reads the row.  All blocks read the same
+// final values; the order of the additions is the memory system's, so a sum
+// may differ from launch to launch in its last bits.  Three rows rotate:
+// after reading row k, block 0 clears row k + 2, which no block reads or
+// writes again before the barrier that precedes the producers of reduction
+// k + 2.
+struct Acc {
+  double* rows;
+  int ld;
+  __device__ __forceinline__ double* row(unsigned int k) const { return rows + (k % 3) * ld; }
+};
+
+__device__ __forceinline__ void acc_add(double* row, int q, double v) { atomicAdd(row + q, v); }
+
+// Maxima are nonnegative or NaN (with the sign bit clear), which order as
+// their bit patterns, NaN above every number.
+__device__ __forceinline__ void acc_max(double* row, int q, double v)
+{
+  atomicMax(reinterpret_cast<unsigned long long*>(row + q), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+// After the grid barrier that follows the producers of reduction k: out[q] =
+// entry q of row k (q < ne) in every block; k advances.
+__device__ __forceinline__ void acc_read(const Acc& A, unsigned int& k, int ne, double* out)
+{
+  const double* r = A.row(k);
+  for (int q = threadIdx.x; q < ne; q += NT) out[q] = __ldcg(r + q);
+  if (blockIdx.x == 0) {
+    double* z = A.row(k + 2);
+    for (int q = threadIdx.x; q < A.ld; q += NT) z[q] = 0.0;
+  }
+  ++k;
+  __syncthreads();
+}
+
+// Adds the sum of the warp partials, in warp order, to entry q of an
+// accumulator row.
+__device__ __forceinline__ void commit_sum(const double* wpart, double* row, int q)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
     for (int w = 0; w < NW; ++w) s += wpart[w];
-    *dst = s;
+    acc_add(row, q, s);
   }
   __syncthreads();
 }
 
 __device__ __forceinline__ double nanmax(double m, double v) { return (m < v || v != v) ? v : m; }
-
-// out[q] for q < nsum + nmax, over the blocks' partial rows: the sum of
-// part[b][q] for q < nsum, the max (NaN propagates) for the nmax entries
-// after them.  Blocks go in fixed groups, each summed in block order by one
-// thread, and the groups in order: every block computes identical values.
-// Threads of a group read consecutive entries of one partial row; every load
-// of a batch is issued before the first add (indices clamped in range, the
-// surplus masked off), so a batch costs one L2 round trip.  Callers enter
-// right after a grid barrier, so no thread still reads out or scratch.
-__device__ __forceinline__ void grid_reduce_redundant(const double* part, int ld, int nsum, int nmax, double* out,
-                                                      double* scratch)
-{
-  constexpr int B = 16;  // loads in flight per thread
-  const int ne = nsum + nmax;
-  const int nb = gridDim.x;
-  int groups = NT / ne;
-  if (groups < 1) groups = 1;
-  if (groups > B) groups = B;
-  const int per = (nb + groups - 1) / groups;
-  for (int t = threadIdx.x; t < ne * groups; t += NT) {
-    const int q = t % ne, gi = t / ne;
-    const bool mx = q >= nsum;
-    const int b0 = gi * per, b1 = b0 + per < nb ? b0 + per : nb;
-    double s = 0.0;
-    for (int c0 = b0; c0 < b1; c0 += B) {
-      double v[B];
-#pragma unroll
-      for (int k = 0; k < B; ++k) v[k] = __ldcg(part + static_cast<long long>(c0 + k < b1 ? c0 + k : b1 - 1) * ld + q);
-#pragma unroll
-      for (int k = 0; k < B; ++k) {
-        const double r = mx ? nanmax(s, v[k]) : s + v[k];
-        s = c0 + k < b1 ? r : s;
-      }
-    }
-    if (ne * groups <= NT) scratch[gi * ne + q] = s;
-    else scratch[q] = s;  // ne > NT: one group
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < ne; q += NT) {
-    const bool mx = q >= nsum;
-    double s = 0.0;
-    if (ne * groups <= NT) {
-      double v[B];
-#pragma unroll
-      for (int gi = 0; gi < B; ++gi) v[gi] = scratch[(gi < groups ? gi : groups - 1) * ne + q];
-#pragma unroll
-      for (int gi = 0; gi < B; ++gi) {
-        const double r = mx ? nanmax(s, v[gi]) : s + v[gi];
-        s = gi < groups ? r : s;
-      }
-    } else {
-      s = scratch[q];
-    }
-    out[q] = s;
-  }
-  __syncthreads();
-}
 
 // sum_{q<k} red[q]^2 by every warp (lanes stride, fixed shuffle tree): the
 // same value in every thread of every block.
@@ -420,18 +403,17 @@ __device__ __forceinline__ double warp_max(double m)
   return m;
 }
 
-// Block max (NaN propagates, marking nonfinite) -> part_row[q].
-__device__ __forceinline__ void block_max_partial(double v, double* part_row, int q, double* scratch)
+// Block max (NaN propagates, marking nonfinite), returned in thread 0.
+__device__ __forceinline__ double block_max(double v, double* scratch)
 {
   v = warp_max(v);
   if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = v;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double m = scratch[0];
+  double m = scratch[0];
+  if (threadIdx.x == 0)
     for (int w = 1; w < NW; ++w) m = nanmax(m, scratch[w]);
-    part_row[q] = m;
-  }
   __syncthreads();
+  return m;
 }
 
 struct SolveState {
@@ -483,14 +465,14 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&s)[DG], int lane)
   return v;
 }
 
-// Dot products of the block's rows: part_row[i] = v_i . w for i < nvec, and
-// with_norm: ||w||^2 -> part_row[nvec], a nonfinite count of w ->
-// part_row[nvec + 1].  Every thread takes part: DG sums a pass over its rows
+// Dot products of the block's rows, added to an accumulator row: entry i
+// += v_i . w for i < nvec, and with_norm: ||w||^2 to entry nvec, a nonfinite
+// count of w to entry nvec + 1.  Every thread takes part: DG sums a pass over its rows
 // (w read once a pass), a reduce-scatter of the DG sums in each warp, then
 // the warps' partials summed in warp order.
 template <typename TV>
 __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __restrict__ w, Rows rw, int nvec,
-                                           bool with_norm, double* part_row, double* dpart)
+                                           bool with_norm, double* row, double* dpart)
 {
   const TV* __restrict__ V = bs.V;
   const long long n = bs.n;
@@ -534,7 +516,7 @@ __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) sm += __shfl_xor_sync(0xffffffffu, sm, o);
-      if (lane == 0) part_row[i] = sm;
+      if (lane == 0) acc_add(row, i, sm);
     }
     __syncthreads();
     return;
@@ -582,7 +564,7 @@ __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __
   for (int i = threadIdx.x; i < tot; i += NT) {
     double t = 0.0;
     for (int wv = 0; wv < NW; ++wv) t += dpart[i * NW + wv];
-    part_row[i] = t;
+    acc_add(row, i, t);
   }
   __syncthreads();
 }
@@ -698,13 +680,11 @@ template <typename TV, bool RES>
 __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec, const double* x0vec, double* xvec,
                              TV* __restrict__ V, double* __restrict__ w,
                              double* __restrict__ rres, int kmax, double tol, double restart_rtol, unsigned int& gen,
-                             double* shbase)
+                             unsigned int& nred, double* shbase)
 {
   const long long n = a.n;
   const Rows rw = own_rows(n);
   const bool wide = rw.r1 - rw.r0 > NT;  // two rows a thread per pass
-  const int ld = a.ld;
-  double* part_row = a.part + static_cast<long long>(blockIdx.x) * ld;
   const Smem S = carve(shbase, a.m);
   // RES = false: no resident vectors (K a constant 0, the shared-memory
   // paths compiled out, the register budget of the plain solve)
@@ -724,15 +704,19 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     if (wide) sweep_r0<2>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
     else sweep_r0<1>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
     warp_partial(r2, S.wpart);
-    commit_partial(S.wpart, part_row);
-    block_max_partial(bmax, part_row, 1, S.scratch);
-    block_max_partial(rmax, part_row, 2, S.scratch);
+    commit_sum(S.wpart, Acc{a.acc, a.ld}.row(nred), 0);
+    bmax = block_max(bmax, S.scratch);
+    rmax = block_max(rmax, S.scratch);
+    if (threadIdx.x == 0) {
+      acc_max(Acc{a.acc, a.ld}.row(nred), 1, bmax);
+      acc_max(Acc{a.acc, a.ld}.row(nred), 2, rmax);
+    }
   }
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
     st.timeout = 1;
     return st;
   }
-  grid_reduce_redundant(a.part, ld, 1, 2, S.red, S.scratch);
+  acc_read(Acc{a.acc, a.ld}, nred, 3, S.red);
   beta = sqrt(S.red[0]);
   const double bn_raw = S.red[1];
   const double r0inf = S.red[2];
@@ -800,8 +784,8 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     if (broke || j >= kmax) {
       // no further column: the test of iterate j on its own
       if (j > 0) {
-        grid_reduce_redundant(a.part + j + 3, ld, 0, 1, S.red, S.scratch);
-        if (check(j, S.red[0])) break;
+        acc_read(Acc{a.acc, a.ld}, nred, j + 4, S.red);
+        if (check(j, S.red[j + 3])) break;
       }
       if (broke) st.breakdown = 1;
       break;
@@ -810,15 +794,15 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     // ---- sweep A: w = A v_j; d_i = v_i . w (i <= j); ||w||^2; nonfinite ----
     if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
     else sweep_spmv<TV, 1>(a.op, rw, vj, w);
-    block_dots<TV>(bs, w, rw, j + 1, true, part_row, S.dpart);
+    block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart);
     if (!grid_sync(a.bar, gen, a.spin_limit)) {
       st.timeout = 1;
       return st;
     }
-    // the dot products and, in the same pass, the residual maxima of iterate
+    // the dot products and, in the same read, the residual maximum of iterate
     // j: the test runs here, one sweep A later than its data, so it costs no
-    // pass of its own (a stopping iterate discards this w)
-    grid_reduce_redundant(a.part, ld, j + 3, j > 0 ? 1 : 0, S.red, S.scratch);
+    // reduction of its own (a stopping iterate discards this w)
+    acc_read(Acc{a.acc, a.ld}, nred, j > 0 ? j + 4 : j + 3, S.red);
     if (j > 0 && check(j, S.red[j + 3])) break;
     if (S.red[j + 2] != 0.0) {
       st.nonfinite = 1;
@@ -841,12 +825,12 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
       if (wide) sweep_combine<TV, true, 2>(rw, bs, S.coef, j + 1, w, w);
       else sweep_combine<TV, true, 1>(rw, bs, S.coef, j + 1, w, w);
-      block_dots<TV>(bs, w, rw, j + 1, true, part_row, S.dpart);
+      block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart);
       if (!grid_sync(a.bar, gen, a.spin_limit)) {
         st.timeout = 1;
         return st;
       }
-      grid_reduce_redundant(a.part, ld, j + 2, 0, S.red, S.scratch);
+      acc_read(Acc{a.acc, a.ld}, nred, j + 2, S.red);
       sw = S.red[j + 1];
       nn2 = sw - sum_squares(S.red, j + 1);
       for (int q = threadIdx.x; q <= j; q += NT) {
@@ -935,7 +919,8 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
                  : sweep_next<TV, 1>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
     }
     st.it = j + 1;
-    block_max_partial(rmx, part_row, j + 4, S.scratch);  // slot (j+1)+3, read after the next sweep A
+    rmx = block_max(rmx, S.scratch);
+    if (threadIdx.x == 0) acc_max(Acc{a.acc, a.ld}.row(nred), j + 4, rmx);  // entry (j+1)+3, read after the next sweep A
   }
   // ---- x = x0 + V_k y_k for the returned iterate k ----
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
@@ -960,13 +945,14 @@ template <bool RES>
 __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
 {
   extern __shared__ double sh[];
-  unsigned int gen = 0;  // barriers passed; the counter is zeroed by the host before the launch
+  unsigned int gen = 0;   // barriers passed; the counter is zeroed by the host before the launch
+  unsigned int nred = 0;  // accumulator reductions completed
   EcgGmresResult out;
   std::memset(&out, 0, sizeof(out));
   const int limit = a.max_iter < a.n ? a.max_iter : static_cast<int>(a.n);
   if (!a.mixed) {
     const SolveState st =
-        krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, sh);
+        krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, nred, sh);
     out.iterations = st.best_it;
     out.converged = st.converged;
     out.breakdown = st.breakdown;
@@ -989,7 +975,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
       const bool last = cycles + 1 >= a.max_refine;
       const int kin = per_cycle < left ? per_cycle : left;
       st = krylov<float, RES>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol, gen,
-                         sh);
+                              nred, sh);
       if (cycles == 0) {
         out.initial_linf = st.r0_linf;
         out.b_linf = st.b_linf;
@@ -1022,7 +1008,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   if (!out.timeout && grid_sync(a.bar, gen, a.spin_limit)) {
     const Rows rw = own_rows(a.n);
     const Smem S = carve(sh, a.m);
-    double* part_row = a.part + static_cast<long long>(blockIdx.x) * a.ld;
+    const Acc A{a.acc, a.ld};
     double rmax = 0.0, bmax = 0.0;
     for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
       const int qq[1] = {q};
@@ -1031,11 +1017,15 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
       rmax = nanmax(rmax, fabs(ax[0] - a.b[q]));
       bmax = nanmax(bmax, fabs(a.b[q]));
     }
-    block_max_partial(rmax, part_row, 0, S.scratch);
-    block_max_partial(bmax, part_row, 1, S.scratch);
+    rmax = block_max(rmax, S.scratch);
+    bmax = block_max(bmax, S.scratch);
+    if (threadIdx.x == 0) {
+      acc_max(A.row(nred), 0, rmax);
+      acc_max(A.row(nred), 1, bmax);
+    }
     if (grid_sync(a.bar, gen, a.spin_limit)) {
       if (blockIdx.x == 0) {
-        grid_reduce_redundant(a.part, a.ld, 0, 2, S.red, S.scratch);
+        acc_read(A, nred, 2, S.red);
         out.final_linf = S.red[0];
         out.final_b_linf = S.red[1];
       }
@@ -1063,8 +1053,12 @@ __global__ void __launch_bounds__(NT) residual_kernel(EcgPressureOp op, long lon
     rmax = nanmax(rmax, fabs(rq));
     bmax = nanmax(bmax, fabs(b[q]));
   }
-  block_max_partial(rmax, part + blockIdx.x * 2, 0, sh);
-  block_max_partial(bmax, part + blockIdx.x * 2, 1, sh);
+  rmax = block_max(rmax, sh);
+  bmax = block_max(bmax, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x * 2] = rmax;
+    part[blockIdx.x * 2 + 1] = bmax;
+  }
 }
 
 }  // namespace
@@ -1079,7 +1073,8 @@ struct EcgGmresWork {
   double* w = nullptr;
   double* r = nullptr;
   float* V32 = nullptr;
-  double* part = nullptr;
+  double* part = nullptr;  // residual_kernel's block maxima
+  double* acc = nullptr;   // three accumulator rows of ld doubles
   int ld = 0;
   double* R = nullptr;
   GridBar* bar = nullptr;
@@ -1141,9 +1136,8 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   else alloc(reinterpret_cast<void**>(&w->V), sizeof(double) * (w->m + 1) * n);
   alloc(reinterpret_cast<void**>(&w->w), sizeof(double) * n);
   alloc(reinterpret_cast<void**>(&w->r), sizeof(double) * n);
-  const long long part_len = static_cast<long long>(w->ld) * w->nblocks;
-  alloc(reinterpret_cast<void**>(&w->part),
-        sizeof(double) * (part_len > 2LL * kResidualBlocks ? part_len : 2LL * kResidualBlocks));
+  alloc(reinterpret_cast<void**>(&w->part), sizeof(double) * 2 * kResidualBlocks);
+  alloc(reinterpret_cast<void**>(&w->acc), sizeof(double) * 3 * w->ld);
   alloc(reinterpret_cast<void**>(&w->R), sizeof(double) * (w->m + 1) * (w->m + 1));
   alloc(reinterpret_cast<void**>(&w->bar), sizeof(GridBar));
   alloc(reinterpret_cast<void**>(&w->d_res), sizeof(EcgGmresResult));
@@ -1180,6 +1174,7 @@ void gmres_work_destroy(EcgGmresWork* w)
   cudaFree(w->r);
   cudaFree(w->V32);
   cudaFree(w->part);
+  cudaFree(w->acc);
   cudaFree(w->R);
   cudaFree(w->bar);
   cudaFree(w->d_res);
@@ -1205,6 +1200,7 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.r = w->r;
   a.V32 = w->V32;
   a.part = w->part;
+  a.acc = w->acc;
   a.R = w->R;
   a.bar = w->bar;
   a.res = w->d_res;
@@ -1221,6 +1217,8 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.prow = w->prow;
   a.spin_limit = 1LL << 25;  // ~2 s of polling before a barrier gives up
   cudaError_t e = cudaMemsetAsync(w->bar, 0, sizeof(GridBar), s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(w->acc, 0, sizeof(double) * 3 * w->ld, s);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
   void* kern = w->kres > 0 ? reinterpret_cast<void*>(gmres_kernel<true>) : reinterpret_cast<void*>(gmres_kernel<false>);
