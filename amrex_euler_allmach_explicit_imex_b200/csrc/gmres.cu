@@ -182,15 +182,16 @@ __device__ __forceinline__ void basis_combine(double (&acc)[R], const Basis<TV>&
                                               int cnt)
 {
   constexpr int B = (sizeof(TV) == 8 ? 32 : 16) / R;
+  constexpr int BS = 8 / R;  // shared-memory loads in flight: their latency is short
   const int ks = cnt < bs.K ? cnt : bs.K;
-  for (int i0 = 0; i0 < ks; i0 += B) {
-    TV a[R][B];
+  for (int i0 = 0; i0 < ks; i0 += BS) {
+    TV a[R][BS];
 #pragma unroll
-    for (int k = 0; k < B; ++k)
+    for (int k = 0; k < BS; ++k)
 #pragma unroll
       for (int r = 0; r < R; ++r) a[r][k] = bs.s[(i0 + k < ks ? i0 + k : ks - 1) * bs.P + q[r] - bs.r0];
 #pragma unroll
-    for (int k = 0; k < B; ++k)
+    for (int k = 0; k < BS; ++k)
       if (i0 + k < ks) {
         const double ck = c[i0 + k];
 #pragma unroll
