@@ -36,6 +36,7 @@ SIGNATURES = {
     "ecg_initialize_state": (C.c_int, [_CTX]),
     "ecg_paper_t1s2_run": (C.c_int, [_CTX, C.POINTER(abi.PaperOptions), C.POINTER(abi.PaperResult)]),
     "ecg_measure_fp64_peak": (C.c_int, [C.c_int32, C.POINTER(C.c_double)]),
+    "ecg_check_grid_barrier_timeout": (C.c_int, [C.c_int32, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ecg_create_slab": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(abi.RunConfig), C.POINTER(abi.GpuOptions), C.c_int32,
                                   C.c_int32, C.c_int32, C.c_int32]),
     "ecg_slab_bind_halo": (C.c_int, [_CTX, C.c_void_p, C.c_void_p]),

@@ -294,6 +294,16 @@ def measure_fp64_peak(device=0):
     return v.value
 
 
+def check_grid_barrier_timeout(spin_limit=4096, device=0):
+    """The GMRES grid barrier's bounded wait (ecg_check_grid_barrier_timeout):
+    returns (blocks that passed the first barrier, blocks whose wait at the
+    second ran out); (4, 3) when the bound works."""
+    first, out = C.c_int32(), C.c_int32()
+    check(load().ecg_check_grid_barrier_timeout(device, spin_limit, C.byref(first), C.byref(out)),
+          "check_grid_barrier_timeout")
+    return first.value, out.value
+
+
 class Batch:
     """Many independent explicit solves of uneven grid sizes advanced together
     (ecg_batch_*): one persistent launch per step for the whole batch, CUDA
@@ -359,6 +369,7 @@ __all__ = [
     "Batch",
     "Context",
     "EcgError",
+    "check_grid_barrier_timeout",
     "compute_admissibility_diagnostics",
     "compute_diagnostics",
     "compute_euler_dt",

@@ -1062,6 +1062,25 @@ __global__ void __launch_bounds__(NT) residual_kernel(EcgPressureOp op, long lon
   }
 }
 
+// The grid barrier's bounded wait, exercised on its own: every block passes
+// barrier 0, then block 0 leaves without arriving at barrier 1, so the
+// others' wait runs out after spin_limit polls.  passed[b] = 1 + (barrier 1
+// passed), 0 if barrier 0 already gave up.
+__global__ void barrier_probe_kernel(GridBar* bar, long long spin_limit, int* passed)
+{
+  unsigned int gen = 0;
+  if (!grid_sync(bar, gen, spin_limit)) {
+    if (threadIdx.x == 0) passed[blockIdx.x] = 0;
+    return;
+  }
+  if (blockIdx.x == 0) {
+    if (threadIdx.x == 0) passed[0] = 1;
+    return;
+  }
+  const bool second = grid_sync(bar, gen, spin_limit);
+  if (threadIdx.x == 0) passed[blockIdx.x] = second ? 2 : 1;
+}
+
 }  // namespace
 
 struct EcgGmresWork {
@@ -1256,4 +1275,35 @@ cudaError_t pressure_residual(EcgGmresWork* w, const EcgPressureOp& op, const do
   *rhs_norm = bm > 1.0 ? bm : 1.0;
   *nonfinite = nf ? 1 : 0;
   return cudaSuccess;
+}
+
+// No counterpart in the reference: the timeout path of the GMRES grid
+// barrier, on 4 blocks of 32 threads (see barrier_probe_kernel).
+extern "C" ecg_status ecg_check_grid_barrier_timeout(int32_t device, int64_t spin_limit, int32_t* passed_first,
+                                                     int32_t* timed_out)
+{
+  if (!passed_first || !timed_out || spin_limit < 1 || spin_limit > (1LL << 25)) return ECG_ERR_BAD_ARG;
+  constexpr int kBlocks = 4;
+  if (cudaSetDevice(device) != cudaSuccess) return ECG_ERR_CUDA;
+  GridBar* bar = nullptr;
+  int* d = nullptr;
+  int h[kBlocks] = {};
+  bool ok = cudaMalloc(&bar, sizeof(GridBar)) == cudaSuccess && cudaMalloc(&d, sizeof(h)) == cudaSuccess &&
+            cudaMemset(bar, 0, sizeof(GridBar)) == cudaSuccess && cudaMemset(d, 0xff, sizeof(h)) == cudaSuccess;
+  if (ok) {
+    barrier_probe_kernel<<<kBlocks, 32>>>(bar, spin_limit, d);
+    ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+         cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess;
+  }
+  cudaFree(bar);
+  cudaFree(d);
+  if (!ok) return ECG_ERR_CUDA;
+  int first = 0, out = 0;
+  for (int b = 0; b < kBlocks; ++b) {
+    first += h[b] >= 1 ? 1 : 0;
+    out += b > 0 && h[b] == 1 ? 1 : 0;
+  }
+  *passed_first = first;
+  *timed_out = out;
+  return ECG_OK;
 }

@@ -491,6 +491,15 @@ ecg_status ecg_slab_pack(ecg_ctx* ctx, double* lo, double* hi);
  * launches), the denominator of the explicit step's FP64 roofline. */
 ecg_status ecg_measure_fp64_peak(int32_t device, double* tflops);
 
+/* No counterpart in the reference: the bounded wait of the GMRES grid barrier
+ * (the only device-side wait here), checked on its own.  4 blocks pass one
+ * barrier; then block 0 leaves without arriving at the next, and the other 3
+ * give up after spin_limit polls (1 .. 2^25) instead of hanging.  Reports how
+ * many blocks passed the first barrier (4) and how many timed out at the
+ * second (3); the device stays usable. */
+ecg_status ecg_check_grid_barrier_timeout(int32_t device, int64_t spin_limit, int32_t* passed_first,
+                                          int32_t* timed_out);
+
 /* ---- adjoint of the explicit step --------------------------------------- */
 /* Vector-Jacobian product of U1 = euler_fv_one_step(U0; dt) with dt held
  * fixed: gU0 = (dU1/dU0)^T gU1.  All arrays are device memory holding 4
