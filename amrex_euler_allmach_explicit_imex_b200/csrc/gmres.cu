@@ -45,6 +45,7 @@ namespace {
 constexpr int NT = 512;
 constexpr int kResidualBlocks = 148 * 2;  // grid of residual_kernel
 constexpr double kEps = 2.220446049250313e-16;
+constexpr int kMinCycle = 16;  // mixed: shortest cycle a restart may end
 
 struct GridBar {
   unsigned int arrive;  // arrivals; the top bit is the timeout flag
@@ -769,7 +770,10 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       st.best_linf = linf;
       return true;
     }
-    if (linf <= rtarget) {
+    // a cycle restarts only once its basis holds kMinCycle vectors: shorter
+    // cycles would pay the restart (a true residual and the iterate's update)
+    // for the few sweeps they save
+    if (linf <= rtarget && j >= kMinCycle) {
       st.restart = 1;
       st.best_it = j;
       st.best_linf = linf;
