@@ -393,6 +393,4 @@ def read_config(source=None):
             raise ConfigError("shock_bubble_mach122 requires domain x=[0,4], y=[0,1].")
         if abs(c.gamma - 1.4) > 1e-14:
             raise ConfigError("shock_bubble_mach122 is a same-gamma ideal-gas test with gamma=1.4.")
-        if c.method != abi.METHOD["explicit"]:
-            raise ConfigError("shock_bubble_mach122 runs the explicit method only.")
     return s

@@ -145,10 +145,15 @@ EcgImexMap imex_map(ecg_ctx* c)
   m.ny = c->grid.ny;
   m.px = c->cfg.is_periodic[0] != 0;
   m.py = c->cfg.is_periodic[1] != 0;
-  m.bubble = c->cfg.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D;
+  const bool mach122 = c->cfg.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122;
+  m.bubble = c->cfg.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D || mach122;
+  m.top_wall = mach122 ? 1 : 0;
   m.gamma = c->cfg.gamma;
-  // shock_density_bubble_post_shock_state, problem_initialization.hpp:51-58
-  const double q[4] = {2.8181818181818183, 1.6064386578049976, 0.0, 5.0};
+  // shock_density_bubble_post_shock_state, problem_initialization.hpp:51-58;
+  // the Mach 1.22 variant (no reference counterpart) has its own inflow state
+  // and the bubble's boundary policy with a wall at the top too
+  double q[4] = {2.8181818181818183, 1.6064386578049976, 0.0, 5.0};
+  if (mach122) mach122_post_shock(c->cfg.gamma, q);
   const double kin = 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2]);
   m.cst[0] = q[0];
   m.cst[1] = q[0] * q[1];
@@ -189,10 +194,6 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
   if (c->cfg.spatial_order != 2) return ECG_ERR_UNSUPPORTED;
   if (c->slab()) {
     c->err = "the IMEX pressure system couples the whole grid: no slab contexts";
-    return ECG_ERR_UNSUPPORTED;
-  }
-  if (c->cfg.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122) {
-    c->err = "the Mach 1.22 shock-bubble configuration runs the explicit method only";
     return ECG_ERR_UNSUPPORTED;
   }
   if (!ensure_state(c)) return ECG_ERR_CUDA;

@@ -10,7 +10,8 @@
 // Index maps and physical-boundary states of the IMEX host grid
 // (imex/imex_source_map_helpers.hpp:70-245).
 struct EcgImexMap {
-  int nx, ny, px, py, bubble, pad;
+  int nx, ny, px, py, bubble;
+  int top_wall;     // the Mach 1.22 variant: a reflecting wall above the last row as well
   double gamma;
   double cst[4];    // bubble post-shock conserved state
   double p_fixed;   // bubble fixed post-shock pressure

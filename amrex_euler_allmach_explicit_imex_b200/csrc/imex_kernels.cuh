@@ -77,6 +77,11 @@ __device__ __forceinline__ Cons state_b(const EcgImexMap& m, const double* __res
       c.my = -c.my;
       return c;
     }
+    if (m.top_wall && !m.py && j >= m.ny) {
+      Cons c = star_at(m, S, ii, m.ny - 1);
+      c.my = -c.my;
+      return c;
+    }
     return star_at(m, S, ii, j);
   }
   return star_at(m, S, i, j);
@@ -109,6 +114,11 @@ __device__ __forceinline__ void m_b(const EcgImexMap& m, const double* __restric
     const int ii = mi(m, i);
     if (!m.py && j < 0) {
       m_at(m, K, ii, 0, m0, m1);
+      m1 = -m1;
+      return;
+    }
+    if (m.top_wall && !m.py && j >= m.ny) {
+      m_at(m, K, ii, m.ny - 1, m0, m1);
       m1 = -m1;
       return;
     }
@@ -890,7 +900,15 @@ __device__ __forceinline__ Cons old_cell(const EcgFvParams& P, const double* __r
         j = 0;
       }
     } else if (j >= ny) {
-      j = P.bc.y_hi == BC_PERIODIC ? wrapi(j, ny) : ny - 1;
+      if (P.bc.y_hi == BC_PERIODIC) {
+        j = wrapi(j, ny);
+      } else if (P.bc.y_hi == BC_REFLECT) {  // the Mach 1.22 variant's top wall
+        j = 2 * ny - 1 - j;
+        j = j < 0 ? 0 : j;
+        flip = true;
+      } else {
+        j = ny - 1;
+      }
     }
     const long long o = static_cast<long long>(j) * P.g.pitch + i;
     Cons c{u[o], u[o + P.g.plane], u[o + 2 * P.g.plane], u[o + 3 * P.g.plane]};

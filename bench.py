@@ -296,9 +296,17 @@ def bubble_imex_kv(nx, ny):
 # Krylov basis no longer fits in L2 (the FP32 basis halves the bytes of the
 # sweeps that dominate there; at 256^2 the solve is bound by barrier latency),
 # and the bubble's IMEX step (a few GMRES iterations a solve)
+def mach122_imex_kv(nx, ny):
+    """The Mach 1.22 bubble on [0,4]x[0,1] with the bubble's IMEX settings."""
+    kv = bubble_imex_kv(nx, ny)
+    kv.update({"euler.problem": "shock_bubble_mach122", "geometry.prob_hi": "4 1"})
+    return kv
+
+
 IMEX_CASES = [("gresho_vortex 256x256 periodic, M=0.01", imex_kv(256, 0.01)),
               ("gresho_vortex 768x768 periodic, M=0.01", imex_kv(768, 0.01)),
-              ("shock_density_bubble_2d 2560x640", bubble_imex_kv(2560, 640))]
+              ("shock_density_bubble_2d 2560x640", bubble_imex_kv(2560, 640)),
+              ("shock_bubble_mach122 2560x640 on [0,4]x[0,1]", mach122_imex_kv(2560, 640))]
 
 
 def imex_leg(dev, stream, steps=3):

@@ -964,6 +964,10 @@ struct Host {
   bool px, py, bubble;
   double gamma;
   std::vector<Cons> cell;
+  // The Mach 1.22 variant (no reference counterpart): the bubble's policy with
+  // its own post-shock inflow state, and a wall at the top as well.
+  bool mach122 = false;
+  Prim post() const { return mach122 ? mach122_post_shock(gamma) : bubble_post_shock(); }
   int row(int i, int j) const { return j * nx + i; }
   int mi(int i) const { return px ? wrap(i, nx) : clampi(i, nx); }
   int mj(int j) const { return py ? wrap(j, ny) : clampi(j, ny); }
@@ -980,16 +984,17 @@ struct Host {
   // source_map_state_at_physical_boundary, :98-115
   Cons state_b(int i, int j) const {
     if (bubble) {
-      if (!px && i < 0) return to_cons(bubble_post_shock(), gamma);
+      if (!px && i < 0) return to_cons(post(), gamma);
       const int ii = mi(i);
       if (!py && j < 0) { Cons c = at(ii, 0); c.my = -c.my; return c; }
+      if (mach122 && !py && j >= ny) { Cons c = at(ii, ny - 1); c.my = -c.my; return c; }
       return at(ii, mj(j));
     }
     return at(i, j);
   }
   // source_map_pressure_at_physical_boundary, :235-245
   double p_b(const std::vector<double>& p, int i, int j) const {
-    if (fixed_p(i)) return bubble_post_shock().p;
+    if (fixed_p(i)) return post().p;
     return p[static_cast<std::size_t>(prow(i, j))];
   }
   // source_map_lagged_momentum_at(_physical_boundary), :293-320
@@ -999,13 +1004,22 @@ struct Host {
   }
   void m_b(const std::vector<double>& k, int i, int j, double& m0, double& m1) const {
     if (bubble) {
-      if (!px && i < 0) { const Cons c = to_cons(bubble_post_shock(), gamma); m0 = c.mx; m1 = c.my; return; }
+      if (!px && i < 0) { const Cons c = to_cons(post(), gamma); m0 = c.mx; m1 = c.my; return; }
       const int ii = mi(i);
       if (!py && j < 0) { m_at(k, ii, 0, m0, m1); m1 = -m1; return; }
+      if (mach122 && !py && j >= ny) { m_at(k, ii, ny - 1, m0, m1); m1 = -m1; return; }
     }
     m_at(k, i, j, m0, m1);
   }
 };
+
+Host imex_host(const ecg_run_config& c, int nx, int ny, const Geo& geo)
+{
+  Host h{nx, ny, geo.per[0], geo.per[1],
+         c.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D || c.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122, c.gamma, {}};
+  h.mach122 = c.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122;
+  return h;
+}
 
 struct Face { double h_hat, energy_flux, hl, hr, ql, qr; int guard, flux_nonfinite; };
 
@@ -1088,7 +1102,7 @@ void build_system(const Host& h, const std::vector<double>& p, const std::vector
       std::vector<std::pair<int, double>> terms;
       auto lhs = [&](int pi, int pj, double coeff) {
         if (h.fixed_p(pi)) {
-          const double c = -coeff * bubble_post_shock().p;
+          const double c = -coeff * h.post().p;
           b += c;
           if (!std::isfinite(c)) ++rnf;
           return;
@@ -1269,11 +1283,11 @@ int imex_step(const ecg_run_config& cfg, Grid& gr, double dt, ecg_imex_diag& d)
   const Geo geo(cfg);
   const int nx = gr.nx, ny = gr.ny, n = nx * ny;
   const double gm1 = cfg.gamma - 1.0;
-  if (is_bubble(cfg)) fill_ghosts(gr, cfg, 0.0);
+  if (is_bubble(cfg) || cfg.problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122) fill_ghosts(gr, cfg, 0.0);
   else fill_outflow(gr, geo);
   Grid sg(nx, ny);
   imex_star(cfg, gr, dt, sg);
-  Host h{nx, ny, geo.per[0], geo.per[1], cfg.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D, cfg.gamma, {}};
+  Host h = imex_host(cfg, nx, ny, geo);
   h.cell.resize(static_cast<std::size_t>(n));
   for (int j = 0; j < ny; ++j)
     for (int i = 0; i < nx; ++i) h.cell[static_cast<std::size_t>(h.row(i, j))] = sg.cons(i, j);
@@ -1684,7 +1698,7 @@ int ecgo_imex_build_system(const ecg_run_config* c, const double* star, const do
 {
   const Geo geo(*c);
   const int nx = c->n_cell[0], ny = c->n_cell[1], n = nx * ny;
-  Host h{nx, ny, geo.per[0], geo.per[1], c->problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D, c->gamma, {}};
+  Host h = imex_host(*c, nx, ny, geo);
   h.cell.resize(static_cast<std::size_t>(n));
   for (int r = 0; r < n; ++r) h.cell[r] = Cons{star[r], star[n + r], star[2 * n + r], star[3 * n + r]};
   std::vector<double> pv(p, p + n), kv(static_cast<std::size_t>(2) * n);
@@ -1707,7 +1721,7 @@ void ecgo_imex_star(const ecg_run_config* c, const double* u, double dt, double*
 {
   Grid g = make_grid(c, u);
   const Geo geo(*c);
-  if (is_bubble(*c)) fill_ghosts(g, *c, 0.0);
+  if (is_bubble(*c) || c->problem == ECG_PROBLEM_SHOCK_BUBBLE_MACH122) fill_ghosts(g, *c, 0.0);
   else fill_outflow(g, geo);
   Grid s(c->n_cell[0], c->n_cell[1]);
   imex_star(*c, g, dt, s);
@@ -1719,7 +1733,7 @@ void ecgo_corrected_momentum(const ecg_run_config* c, const double* star, const 
 {
   const Geo geo(*c);
   const int nx = c->n_cell[0], ny = c->n_cell[1], n = nx * ny;
-  Host h{nx, ny, geo.per[0], geo.per[1], c->problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_2D, c->gamma, {}};
+  Host h = imex_host(*c, nx, ny, geo);
   h.cell.resize(static_cast<std::size_t>(n));
   for (int r = 0; r < n; ++r) h.cell[r] = Cons{star[r], star[n + r], star[2 * n + r], star[3 * n + r]};
   const std::vector<double> km = corrected_momentum(h, std::vector<double>(p, p + n), dt, 1.0 / geo.dx, 1.0 / geo.dy);
