@@ -26,8 +26,12 @@
 // column, the rotations and the residual recurrence stay FP64, so the basis
 // rounding is the only FP32 error (a compressed-basis GMRES).  The solve
 // restarts from the current iterate whenever the recurrence says the cycle
-// converged or its residual fell by inner_rtol, and every cycle opens with the
-// true FP64 residual b - A x: the reference's stopping rule is applied to it.
+// converged, or its residual fell by inner_rtol after at least kMinCycle
+// iterations, and every cycle opens with the true FP64 residual b - A x: the
+// reference's stopping rule is applied to it.  These cycles take the DGKS
+// second pass only under severe cancellation (option reorth).
+// Small systems keep the first basis vectors resident in shared memory on
+// each block's rows (the RES instantiation of the kernel).
 #include <cuda_runtime.h>
 
 #include <cmath>
