@@ -1291,20 +1291,30 @@ extern "C" ecg_status ecg_check_grid_barrier_timeout(int32_t device, int64_t spi
                                                      int32_t* timed_out)
 {
   if (!passed_first || !timed_out || spin_limit < 1 || spin_limit > (1LL << 25)) return ECG_ERR_BAD_ARG;
-  constexpr int kBlocks = 4;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return ECG_ERR_NO_DEVICE;
+  int prev = 0;
+  cudaGetDevice(&prev);
   if (cudaSetDevice(device) != cudaSuccess) return ECG_ERR_CUDA;
+  constexpr int kBlocks = 4;
   GridBar* bar = nullptr;
   int* d = nullptr;
+  cudaStream_t s = nullptr;
   int h[kBlocks] = {};
-  bool ok = cudaMalloc(&bar, sizeof(GridBar)) == cudaSuccess && cudaMalloc(&d, sizeof(h)) == cudaSuccess &&
-            cudaMemset(bar, 0, sizeof(GridBar)) == cudaSuccess && cudaMemset(d, 0xff, sizeof(h)) == cudaSuccess;
+  bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&bar, sizeof(GridBar)) == cudaSuccess && cudaMalloc(&d, sizeof(h)) == cudaSuccess &&
+            cudaMemsetAsync(bar, 0, sizeof(GridBar), s) == cudaSuccess &&
+            cudaMemsetAsync(d, 0xff, sizeof(h), s) == cudaSuccess;
   if (ok) {
-    barrier_probe_kernel<<<kBlocks, 32>>>(bar, spin_limit, d);
-    ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
-         cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess;
+    barrier_probe_kernel<<<kBlocks, 32, 0, s>>>(bar, spin_limit, d);
+    ok = cudaGetLastError() == cudaSuccess &&
+         cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaStreamSynchronize(s) == cudaSuccess;
   }
   cudaFree(bar);
   cudaFree(d);
+  if (s) cudaStreamDestroy(s);
+  cudaSetDevice(prev);
   if (!ok) return ECG_ERR_CUDA;
   int first = 0, out = 0;
   for (int b = 0; b < kBlocks; ++b) {

@@ -35,3 +35,8 @@ def test_barrier_check_rejects_unbounded_limits(gpu):
     for bad in (0, -1, (1 << 25) + 1):
         with pytest.raises(api.EcgError):
             api.check_grid_barrier_timeout(spin_limit=bad)
+
+
+def test_barrier_check_rejects_a_missing_device(gpu):
+    with pytest.raises(api.EcgError):
+        api.check_grid_barrier_timeout(device=1 << 20)
