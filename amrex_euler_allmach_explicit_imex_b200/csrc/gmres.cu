@@ -223,6 +223,38 @@ __device__ __forceinline__ void basis_combine(double (&acc)[R], const Basis<TV>&
   }
 }
 
+// basis_combine for the FP32 basis of an even-sized system on the row pair
+// q, q+1 (q even): one 8-byte load per vector and pair, so twice the bytes
+// in flight for the same loads.  Resident vectors come from shared memory.
+template <bool SUB>
+__device__ __forceinline__ void basis_combine_pair(double (&acc)[2], const Basis<float>& bs, int q, const double* c,
+                                                   int cnt)
+{
+  constexpr int B = 16;
+  const int ks = cnt < bs.K ? cnt : bs.K;
+  for (int i = 0; i < ks; ++i) {
+    const double ck = c[i];
+    const float* sv = bs.s + i * bs.P + q - bs.r0;
+    acc[0] = SUB ? acc[0] - ck * static_cast<double>(sv[0]) : acc[0] + ck * static_cast<double>(sv[0]);
+    acc[1] = SUB ? acc[1] - ck * static_cast<double>(sv[1]) : acc[1] + ck * static_cast<double>(sv[1]);
+  }
+  const float* __restrict__ V = bs.V;
+  const long long n = bs.n;
+  for (int i0 = ks; i0 < cnt; i0 += B) {
+    float2 a[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+      a[k] = __ldcg(reinterpret_cast<const float2*>(V + static_cast<long long>(i0 + k < cnt ? i0 + k : cnt - 1) * n + q));
+#pragma unroll
+    for (int k = 0; k < B; ++k)
+      if (i0 + k < cnt) {
+        const double ck = c[i0 + k];
+        acc[0] = SUB ? acc[0] - ck * static_cast<double>(a[k].x) : acc[0] + ck * static_cast<double>(a[k].x);
+        acc[1] = SUB ? acc[1] - ck * static_cast<double>(a[k].y) : acc[1] + ck * static_cast<double>(a[k].y);
+      }
+  }
+}
+
 // Rows q_r = j nx + i of A v with A the source-map pressure operator
 // (imex_source_map_helpers.hpp:533-543), in FP64 whatever the storage of v,
 // R rows with every load issued before the arithmetic (indices are always in
@@ -278,9 +310,15 @@ __device__ __forceinline__ void apply_rows(const EcgPressureOp& op, const TV* __
 struct Rows {
   int r0, r1;
 };
+// Rows of a block: an even count (so row pairs of an even-sized system stay
+// 8-byte aligned in an FP32 basis), the last block taking what is left.
+__host__ __device__ constexpr long long rows_per_block(long long n, int nblocks)
+{
+  return ((n + nblocks - 1) / nblocks + 1) / 2 * 2;
+}
 __device__ __forceinline__ Rows own_rows(long long n)
 {
-  const long long per = (n + gridDim.x - 1) / gridDim.x;
+  const long long per = rows_per_block(n, gridDim.x);
   long long r0 = per * blockIdx.x, r1 = r0 + per;
   if (r1 > n) r1 = n;
   if (r0 > n) r0 = n;
@@ -478,7 +516,7 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&s)[DG], int lane)
 // the warps' partials summed in warp order.
 template <typename TV>
 __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __restrict__ w, Rows rw, int nvec,
-                                           bool with_norm, double* row, double* dpart)
+                                           bool with_norm, double* row, double* dpart, bool pair)
 {
   const TV* __restrict__ V = bs.V;
   const long long n = bs.n;
@@ -531,11 +569,14 @@ __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __
     double s[DG];
 #pragma unroll
     for (int k = 0; k < DG; ++k) s[k] = 0.0;
-    // FP64 basis: two rows a pass (2 DG loads in flight); FP32: one (measured faster)
+    // FP64 basis: two rows a pass (2 DG loads in flight); FP32: one, or with
+    // pair (an even-sized system) the adjacent rows q, q+1 in one 8-byte load
     constexpr int RS = sizeof(TV) == 8 ? 2 : 1;
-    for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += RS * NT) {
-      const bool hb = RS == 2 && q + NT < rw.r1;
-      const int qb = hb ? q + NT : q;
+    const bool pr = sizeof(TV) == 4 && pair;
+    const int qstep = pr ? 2 * NT : RS * NT;
+    for (int q = rw.r0 + (pr ? 2 : 1) * static_cast<int>(threadIdx.x); q < rw.r1; q += qstep) {
+      const bool hb = pr || (RS == 2 && q + NT < rw.r1);
+      const int qb = pr ? q + 1 : (hb ? q + NT : q);
       const double wq[2] = {w[q], hb ? w[qb] : 0.0};
       TV a[2][DG];
       if (g0 + DG <= bs.K) {  // a group of resident vectors
@@ -543,6 +584,16 @@ __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __
         for (int k = 0; k < DG; ++k) {
           a[0][k] = bs.s[(g0 + k) * bs.P + q - rw.r0];
           a[1][k] = hb ? bs.s[(g0 + k) * bs.P + qb - rw.r0] : TV(0);
+        }
+      } else if (pr) {
+        if constexpr (sizeof(TV) == 4) {
+#pragma unroll
+          for (int k = 0; k < DG; ++k) {
+            const float2 v = __ldcg(reinterpret_cast<const float2*>(
+                V + static_cast<long long>(g0 + k < nvec ? g0 + k : nvec - 1) * n + q));
+            a[0][k] = v.x;
+            a[1][k] = v.y;
+          }
         }
       } else {
 #pragma unroll
@@ -641,6 +692,29 @@ __device__ __forceinline__ void sweep_combine(Rows rw, const Basis<TV>& bs, cons
   }
 }
 
+// sweep_next on row pairs (FP32 basis, even-sized system): thread t takes
+// rows r0 + 2t, r0 + 2t + 1, then 2 NT rows further.
+__device__ __forceinline__ double sweep_next_pair(Rows rw, const Basis<float>& bs, const double* c, int cnt,
+                                                  const double* __restrict__ w, double inv_nn, double cr1, double cr2,
+                                                  double* __restrict__ rres)
+{
+  double rmx = 0.0;
+  for (int q = rw.r0 + 2 * static_cast<int>(threadIdx.x); q < rw.r1; q += 2 * NT) {
+    double acc[2] = {w[q], w[q + 1]};
+    const double rp[2] = {rres[q], rres[q + 1]};
+    basis_combine_pair<true>(acc, bs, q, c, cnt);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const float vq = static_cast<float>(acc[r] * inv_nn);
+      bs.store(cnt, q + r, vq);
+      const double rq = cr1 * rp[r] + cr2 * static_cast<double>(vq);
+      rres[q + r] = rq;
+      rmx = nanmax(rmx, fabs(rq));
+    }
+  }
+  return rmx;
+}
+
 // w - V c -> v_cnt = (w - V c) inv_nn (stored as TV), and the residual
 // recurrence rres <- cr1 rres + cr2 v_cnt; returns the block-local max |rres|.
 template <typename TV, int R>
@@ -691,6 +765,8 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   const long long n = a.n;
   const Rows rw = own_rows(n);
   const bool wide = rw.r1 - rw.r0 > NT;  // two rows a thread per pass
+  // FP32 basis of an even-sized system: adjacent row pairs, 8-byte loads
+  const bool pair = sizeof(TV) == 4 && wide && (n & 1) == 0;
   const Smem S = carve(shbase, a.m);
   // RES = false: no resident vectors (K a constant 0, the shared-memory
   // paths compiled out, the register budget of the plain solve)
@@ -803,7 +879,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     // ---- sweep A: w = A v_j; d_i = v_i . w (i <= j); ||w||^2; nonfinite ----
     if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
     else sweep_spmv<TV, 1>(a.op, rw, vj, w);
-    block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart);
+    block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart, pair);
     if (!grid_sync(a.bar, gen, a.spin_limit)) {
       st.timeout = 1;
       return st;
@@ -834,7 +910,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
       if (wide) sweep_combine<TV, true, 2>(rw, bs, S.coef, j + 1, w, w);
       else sweep_combine<TV, true, 1>(rw, bs, S.coef, j + 1, w, w);
-      block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart);
+      block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart, pair);
       if (!grid_sync(a.bar, gen, a.spin_limit)) {
         st.timeout = 1;
         return st;
@@ -924,8 +1000,15 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
         rmx = nanmax(rmx, fabs(rq));
       }
     } else {
-      rmx = wide ? sweep_next<TV, 2>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres)
-                 : sweep_next<TV, 1>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
+      if constexpr (sizeof(TV) == 4) {
+        if (pair) rmx = sweep_next_pair(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
+        else
+          rmx = wide ? sweep_next<TV, 2>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres)
+                     : sweep_next<TV, 1>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
+      } else {
+        rmx = wide ? sweep_next<TV, 2>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres)
+                   : sweep_next<TV, 1>(rw, bs, S.coef, j + 1, w, inv_nn, cr1, cr2, rres);
+      }
     }
     st.it = j + 1;
     rmx = block_max(rmx, S.scratch);
@@ -1135,7 +1218,7 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   // The shared memory left over by the fixed part holds the first basis
   // vectors on the block's rows (one block per SM, so the whole opt-in
   // budget is the block's).
-  w->prow = static_cast<int>((n + w->nblocks - 1) / w->nblocks);
+  w->prow = static_cast<int>(rows_per_block(n, w->nblocks));
   int optin = 0;
   cudaFuncAttributes fa;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||

@@ -328,7 +328,7 @@ def imex_leg(dev, stream, steps=3):
             with api.Context(cfg, imex_precision=prec, device=dev.index or 0, stream=stream.cuda_stream) as ctx:
                 api.initialize_state(ctx)
                 t = 0.0
-                ms, its = [], []
+                ms, its, statuses = [], [], []
                 for k in range(steps + 1):
                     dt, _ = api.compute_imex_dt(ctx, t)
                     a = torch.cuda.Event(enable_timing=True)
@@ -337,13 +337,14 @@ def imex_leg(dev, stream, steps=3):
                     d = api.euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, dt)
                     b.record(stream)
                     b.synchronize()
+                    statuses.append(api.solver_status_str(d.solver_status))
                     if k > 0:
                         ms.append(a.elapsed_time(b))
                         its.append(d.gmres_inner_iterations if prec == "mixed" else d.solver_iterations)
                     t += dt
                 states[prec] = ctx.download()
                 out[prec] = {"ms_per_step": statistics.median(ms), "gmres_iterations": its,
-                             "status": api.solver_status_str(d.solver_status)}
+                             "status": api.solver_status_str(d.solver_status), "step_statuses": statuses}
         drift = float(np.abs(states["fp64"] - states["mixed"]).max() / np.abs(states["fp64"]).max())
         cases.append({"workload": name + ", IMEX T1/S2, 4 Picard, GMRES tol 1e-10", "fp64": out["fp64"],
                       "mixed": out["mixed"], "mixed_speedup": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
