@@ -1033,7 +1033,9 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   return st;
 }
 
-template <bool RES>
+// One instantiation per (resident basis, basis precision): the FP64 and the
+// FP32-basis solves each get the registers of their own path.
+template <bool RES, bool MIXED>
 __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
 {
   extern __shared__ double sh[];
@@ -1042,7 +1044,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   EcgGmresResult out;
   std::memset(&out, 0, sizeof(out));
   const int limit = a.max_iter < a.n ? a.max_iter : static_cast<int>(a.n);
-  if (!a.mixed) {
+  if constexpr (!MIXED) {
     const SolveState st =
         krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, nred, sh);
     out.iterations = st.best_it;
@@ -1172,6 +1174,16 @@ __global__ void barrier_probe_kernel(GridBar* bar, long long spin_limit, int* pa
   if (threadIdx.x == 0) passed[blockIdx.x] = second ? 2 : 1;
 }
 
+// The kernel instantiation for a workspace: with or without the resident
+// basis, FP64 or FP32 basis.
+const void* gmres_entry(bool res, bool mixed)
+{
+  if (res) return mixed ? reinterpret_cast<const void*>(gmres_kernel<true, true>)
+                        : reinterpret_cast<const void*>(gmres_kernel<true, false>);
+  return mixed ? reinterpret_cast<const void*>(gmres_kernel<false, true>)
+               : reinterpret_cast<const void*>(gmres_kernel<false, false>);
+}
+
 }  // namespace
 
 struct EcgGmresWork {
@@ -1222,7 +1234,7 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   int optin = 0;
   cudaFuncAttributes fa;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
-      cudaFuncGetAttributes(&fa, gmres_kernel<true>) != cudaSuccess) {
+      cudaFuncGetAttributes(&fa, gmres_entry(true, mixed)) != cudaSuccess) {
     if (err) *err = "gmres kernel attributes unavailable";
     delete w;
     return nullptr;
@@ -1256,14 +1268,13 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   if (ok && cudaMallocHost(&w->h_part, sizeof(double) * 2 * kResidualBlocks) != cudaSuccess) ok = false;
   if (ok && cudaMemset(w->bar, 0, sizeof(GridBar)) != cudaSuccess) ok = false;
   // the whole budget, so workspaces of any size can launch
-  if (ok && (cudaFuncSetAttribute(gmres_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(budget)) != cudaSuccess ||
-             cudaFuncSetAttribute(gmres_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(budget)) != cudaSuccess))
-    ok = false;
+  for (int v = 0; v < 4 && ok; ++v)
+    if (cudaFuncSetAttribute(gmres_entry(v & 1, v & 2), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(budget)) != cudaSuccess)
+      ok = false;
   int per_sm = 0;
-  if (ok && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, w->kres > 0 ? gmres_kernel<true> : gmres_kernel<false>,
-                                                           NT, w->smem) != cudaSuccess ||
+  if (ok && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_entry(w->kres > 0, mixed), NT, w->smem) !=
+                 cudaSuccess ||
              per_sm < 1)) {
     if (err) *err = "gmres kernel does not fit on one SM with its shared memory";
     gmres_work_destroy(w);
@@ -1332,8 +1343,7 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   e = cudaMemsetAsync(w->acc, 0, sizeof(double) * 3 * w->ld, s);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
-  void* kern = w->kres > 0 ? reinterpret_cast<void*>(gmres_kernel<true>) : reinterpret_cast<void*>(gmres_kernel<false>);
-  e = cudaLaunchCooperativeKernel(kern, dim3(w->nblocks), dim3(NT), args, w->smem, s);
+  e = cudaLaunchCooperativeKernel(gmres_entry(w->kres > 0, w->mixed), dim3(w->nblocks), dim3(NT), args, w->smem, s);
   if (e != cudaSuccess) return e;
   e = cudaMemcpyAsync(w->h_res, w->d_res, sizeof(EcgGmresResult), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return e;
