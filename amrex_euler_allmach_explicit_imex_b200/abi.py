@@ -75,6 +75,7 @@ class GpuOptions(C.Structure):
         ("tile_y", C.c_int32),
         ("mixed_reorth", C.c_int32),
         ("stream", C.c_void_p),
+        ("deterministic", C.c_int32),
     ]
 
 
@@ -158,6 +159,7 @@ IMEX_DIAG_REAL_FIELDS = [
     "eq78_divergence_scaled_linf",
     "energy_closeout_delta_l1",
     "energy_closeout_delta_linf",
+    "gmres_vector_bytes",
 ]
 
 

@@ -392,7 +392,7 @@ ecg_status ecg_create(ecg_ctx** out, const ecg_run_config* cfg, const ecg_gpu_op
   // kernel choice: 0 default (fast build: column-strip kernel with paired
   // faces; exact build: 32x16 tile), 2 column strips with faces one at a time,
   // 1 square 16x16 tile (fast build), 8 or 16: 32xTY tile
-  c->tile_y = (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
+  c->tile_y = (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 3 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
   const size_t sbytes = sizeof(double) * 4 * c->grid.plane;
   bool ok = true;
   if (o.stream) {
@@ -575,7 +575,7 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
   const int nx = c->grid.nx, ny = c->grid.ny;
   if (lo_x > 0 || lo_y > 0 || jstride < nx - lo_x || nstride < jstride * (ny - lo_y)) return ECG_ERR_BAD_ARG;
   EcgFvParams p = fv_params(c, false);
-  const bool banded = c->opt.arith == ECG_ARITH_FAST && (c->tile_y == 0 || c->tile_y == 2) && !c->slab() &&
+  const bool banded = c->opt.arith == ECG_ARITH_FAST && (c->tile_y == 0 || c->tile_y == 2 || c->tile_y == 3) && !c->slab() &&
                       c->cfg.riemann != ECG_RIEMANN_XIE_AM_HLLC_P && !p.bc.ring && ny >= 32;
   if (!banded) {
     ecg_status st = ecg_upload_state(c, in, lo_x, lo_y, jstride, nstride);

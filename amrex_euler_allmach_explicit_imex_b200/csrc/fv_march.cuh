@@ -206,14 +206,175 @@ __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* 
   }
 }
 
+// ---- the staged march: rows reach the warp through shared memory --------
+//
+// Each warp keeps the conserved values of the rows it is about to use in a
+// ring of kRing rows in shared memory (slot = row mod kRing, component planes
+// of 32 lanes).  A lane requests the cell of its column kAhead rows ahead of
+// the one being converted with cp.async (8 bytes per component, straight
+// from the state, the exact-Dirichlet ring or a slab halo, whichever the
+// ghost policy names); constant ghost states are stored directly.  The load
+// latency of a row is thus hidden behind kAhead rows of flux work without
+// holding registers, and the old state of the updated row is read back from
+// the ring instead of from global memory.  Each lane only reads the slots it
+// wrote itself, so cp.async.wait_group is the only synchronisation.
+constexpr int kRing = 8;
+constexpr int kAhead = 4;
+static_assert(kAhead + 4 <= kRing, "the prologue stages rows j0-2 .. j0+1+kAhead");
+
+struct StageRing {
+  double v[kRing][4][kLanes];
+};
+
+__device__ __forceinline__ void cp_async8(unsigned dst, const double* src)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int RK, int LIM, bool PAIR>
+__device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const double* __restrict__ u,
+                                                   double* __restrict__ out, int c0, int j0, int H, double dt,
+                                                   bool count_deg, MarchAcc& acc, StageRing& ring)
+{
+  const int lane = threadIdx.x & 31;
+  const int x = c0 - 2 + lane;
+  const int nx = P.g.nx, ny = P.g.ny;
+  const double g = P.gamma, inv_gm1 = fast::frcp(g - 1.0);
+  const double idx = P.g.inv_dx, idy = P.g.inv_dy;
+  const bool second = P.order > 1;
+  const bool inner = lane >= 2 && lane < 2 + kCells;
+  const bool cell_ok = inner && x < nx;
+  const bool xface = lane >= 2 && lane <= 2 + kCells;
+  const int xs = x < 0 ? 0 : (x < nx ? x : nx - 1);
+  const int rhi = P.row_hi > 0 && P.row_hi < ny ? P.row_hi : ny;
+  const int jend = j0 + H < rhi ? j0 + H : rhi;
+  const int jlast = jend + 1;  // the last row the strip reads
+
+  double* const col = &ring.v[0][0][lane];
+  const unsigned col_s = static_cast<unsigned>(__cvta_generic_to_shared(col));
+  unsigned flips = 0;  // bit (row mod kRing): that staged row is a mirror image (my to negate)
+  // request row jr of this lane's column (an empty group past the strip's rows)
+  auto put = [&](int jr) {
+    if (jr <= jlast) {
+      const int sl = jr & (kRing - 1);
+      const CellSrc c = cell_src(P, u, x, jr);
+      flips = c.flip ? (flips | (1u << sl)) : (flips & ~(1u << sl));
+      if (c.p) {
+        const unsigned d = col_s + static_cast<unsigned>(sl * 4 * kLanes * 8);
+        cp_async8(d, c.p);
+        cp_async8(d + kLanes * 8, c.p + c.pl);
+        cp_async8(d + 2 * kLanes * 8, c.p + 2 * c.pl);
+        cp_async8(d + 3 * kLanes * 8, c.p + 3 * c.pl);
+      } else {
+        double* d = col + sl * 4 * kLanes;
+        d[0] = P.bc.cst[0];
+        d[kLanes] = P.bc.cst[1];
+        d[2 * kLanes] = P.bc.cst[2];
+        d[3 * kLanes] = P.bc.cst[3];
+      }
+    }
+    cp_async_commit();
+  };
+  auto get = [&](int jr) {
+    const int sl = jr & (kRing - 1);
+    const double* d = col + sl * 4 * kLanes;
+    Cons c{d[0], d[kLanes], d[2 * kLanes], d[3 * kLanes]};
+    if ((flips >> sl) & 1u) c.my = -c.my;
+    return c;
+  };
+
+  // ---- prologue: stage rows j0-2 .. j0+1+kAhead; rows j0-2 .. j0+1 first ----
+#pragma unroll
+  for (int r = -2; r <= 1 + kAhead; ++r) put(j0 + r);
+  cp_async_wait<kAhead>();
+  Prim q_m2 = fast::to_prim_f(get(j0 - 2), g);
+  Lane L;
+  L.q[1] = fast::to_prim_f(get(j0 - 1), g);
+  L.q[2] = fast::to_prim_f(get(j0), g);
+  L.q[3] = fast::to_prim_f(get(j0 + 1), g);
+  const Prim sy_m1 = slope3<LIM>(q_m2, L.q[1], L.q[2], second);
+  Prim sy_cur = slope3<LIM>(L.q[1], L.q[2], L.q[3], second);
+  Cons gb;
+  {
+    bool deg;
+    gb = face_one<RK>(plus_half(L.q[1], sy_m1), minus_half(L.q[2], sy_cur), 1, g, inv_gm1, deg);
+    if (count_deg && deg && cell_ok && j0 < ny) acc.degenerate += 1;
+  }
+  const long long pl = P.g.plane;
+  double* orow = out + static_cast<long long>(j0) * P.g.pitch + xs;
+  for (int j = j0; j < jend; ++j, orow += P.g.pitch) {
+    put(j + 2 + kAhead);
+    cp_async_wait<kAhead>();  // row j + 2 has landed
+    L.q[1] = L.q[2];
+    L.q[2] = L.q[3];
+    L.q[3] = fast::to_prim_f(get(j + 2), g);
+    const Prim& qc = L.q[1];
+    const Prim sy_next = slope3<LIM>(L.q[1], L.q[2], L.q[3], second);
+    const Prim ql{shup(qc.rho), shup(qc.u), shup(qc.v), shup(qc.p)};
+    const Prim qr{shdn(qc.rho), shdn(qc.u), shdn(qc.v), shdn(qc.p)};
+    const Prim sx = slope3<LIM>(ql, qc, qr, second);
+    const Prim sxl{shup(sx.rho), shup(sx.u), shup(sx.v), shup(sx.p)};
+    Cons fl, gt;
+    bool deg_x, deg_y;
+    if (PAIR) {
+      face_pair<RK>(plus_half(ql, sxl), minus_half(qc, sx), plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), g,
+                    inv_gm1, fl, gt, deg_x, deg_y);
+    } else {
+      gt = face_w<RK>(plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), 1, g, inv_gm1, deg_y);
+      fl = face_w<RK>(plus_half(ql, sxl), minus_half(qc, sx), 0, g, inv_gm1, deg_x);
+    }
+    const Cons fr{shdn(fl.rho), shdn(fl.mx), shdn(fl.my), shdn(fl.E)};
+    if (count_deg) {
+      // each face counts once per adjacent cell of this strip in the domain
+      // (count_hllc_degenerate_star_states, explicit_update.hpp:2-56)
+      const bool left_ok = lane >= 3 && lane <= 2 + kCells && x - 1 < nx;
+      if (deg_x && xface) acc.degenerate += (left_ok ? 1 : 0) + (cell_ok ? 1 : 0);
+      if (deg_y && cell_ok) acc.degenerate += 1 + (j + 1 < jend ? 1 : 0);
+    }
+    // update (explicit_update.hpp:92-95) from the staged old state of row j
+    const Cons old = get(j);
+    Cons n;
+    n.rho = old.rho - dt * ((fr.rho - fl.rho) * idx + (gt.rho - gb.rho) * idy);
+    n.mx = old.mx - dt * ((fr.mx - fl.mx) * idx + (gt.mx - gb.mx) * idy);
+    n.my = old.my - dt * ((fr.my - fl.my) * idx + (gt.my - gb.my) * idy);
+    n.E = old.E - dt * ((fr.E - fl.E) * idx + (gt.E - gb.E) * idy);
+    const Prim q = fast::to_prim_f(n, g);
+    const double cs = fast::fsound_w(q.rho, q.p, g);
+    if (cell_ok) {
+      orow[0] = n.rho;
+      orow[pl] = n.mx;
+      orow[2 * pl] = n.my;
+      orow[3 * pl] = n.E;
+      const double rate = (fabs(q.u) + cs) * idx + (fabs(q.v) + cs) * idy;
+      if (!isnan(rate)) acc.kmax = umax64(acc.kmax, okey(rate));
+      const bool bad = !isfinite(q.rho) || !isfinite(q.u) || !isfinite(q.v) || !isfinite(q.p) || !isfinite(n.E);
+      acc.krho = umin64(acc.krho, okey(bad ? -kInf : q.rho));
+      acc.kp = umin64(acc.kp, okey(bad ? -kInf : q.p));
+      acc.nonfinite += bad ? 1 : 0;
+    }
+    gb = gt;
+    sy_cur = sy_next;
+  }
+  cp_async_wait<0>();  // no request outlives the strip
+}
+
 // At most 128 registers a thread (4 blocks of 4 warps per SM): measured
 // faster than the 166-register schedule the paired faces get unbounded.
-template <int RK, int LIM, int WPB, bool PAIR>
+// STAGE: rows through the shared-memory ring (march_strip_staged), else
+// straight from global memory into registers (march_strip).
+template <int RK, int LIM, int WPB, bool PAIR, bool STAGE>
 __global__ void __launch_bounds__(WPB * 32, 16 / WPB)
 fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __restrict__ out,
                 EcgStepStats* __restrict__ stats, const EcgDtCtl ctl, const int H)
 {
   __shared__ BlockRed<WPB * 32> red;
+  __shared__ StageRing ring[STAGE ? WPB : 1];
   const int strip = blockIdx.x * WPB + (threadIdx.x >> 5);
   const int c0 = strip * kCells;
   const int j0 = (P.row_hi > 0 ? P.row_lo : 0) + blockIdx.y * H;
@@ -223,14 +384,20 @@ fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __res
 
   MarchAcc acc;
   acc.init();
-  if (c0 < P.g.nx) march_strip<RK, LIM, PAIR>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc);
+  if (c0 < P.g.nx) {
+    if (STAGE)
+      march_strip_staged<RK, LIM, PAIR>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc,
+                                        ring[STAGE ? threadIdx.x >> 5 : 0]);
+    else
+      march_strip<RK, LIM, PAIR>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc);
+  }
   block_commit<WPB * 32>(red, acc.kmax, acc.krho, acc.kp, acc.nonfinite, acc.degenerate, &stats[ctl.acc_slot]);
 }
 
 // Rows per warp: the given march_rows, else the smallest count that lets all
 // warp strips of the grid run in a single wave of resident warps (so no SM
 // idles in a tail), at least 8 so the per-strip prologue stays cheap.
-template <int RK, int LIM, bool PAIR>
+template <int RK, int LIM, bool PAIR, bool STAGE>
 cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
                        cudaStream_t s)
 {
@@ -246,7 +413,8 @@ cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgS
     static int blocks_per_sm = 0;
     if (blocks_per_sm == 0) {
       int b = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fv_march_kernel<RK, LIM, WPB, PAIR>, WPB * 32, 0) != cudaSuccess ||
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fv_march_kernel<RK, LIM, WPB, PAIR, STAGE>, WPB * 32, 0) !=
+              cudaSuccess ||
           b < 1)
         b = 1;
       blocks_per_sm = b;
@@ -257,37 +425,40 @@ cudaError_t launch_lim(const EcgFvParams& p, const double* in, double* out, EcgS
     if (H < 8) H = 8;
   }
   const dim3 grid((strips + WPB - 1) / WPB, (rows + H - 1) / H);
-  fv_march_kernel<RK, LIM, WPB, PAIR><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl, H);
+  fv_march_kernel<RK, LIM, WPB, PAIR, STAGE><<<grid, WPB * 32, 0, s>>>(p, in, out, stats, ctl, H);
   return cudaGetLastError();
 }
 
-template <int RK, bool PAIR>
+template <int RK, bool PAIR, bool STAGE>
 cudaError_t launch_rk(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
                       cudaStream_t s)
 {
   switch (p.limiter) {
-    case ECG_LIMITER_MC: return launch_lim<RK, ECG_LIMITER_MC, PAIR>(p, in, out, stats, ctl, s);
-    case ECG_LIMITER_VANLEER: return launch_lim<RK, ECG_LIMITER_VANLEER, PAIR>(p, in, out, stats, ctl, s);
-    default: return launch_lim<RK, ECG_LIMITER_MINMOD, PAIR>(p, in, out, stats, ctl, s);
+    case ECG_LIMITER_MC: return launch_lim<RK, ECG_LIMITER_MC, PAIR, STAGE>(p, in, out, stats, ctl, s);
+    case ECG_LIMITER_VANLEER: return launch_lim<RK, ECG_LIMITER_VANLEER, PAIR, STAGE>(p, in, out, stats, ctl, s);
+    default: return launch_lim<RK, ECG_LIMITER_MINMOD, PAIR, STAGE>(p, in, out, stats, ctl, s);
   }
 }
 
+template <int RK>
+cudaError_t launch_mode(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats, const EcgDtCtl& ctl,
+                        cudaStream_t s, bool pair, bool stage)
+{
+  if (stage) return launch_rk<RK, true, true>(p, in, out, stats, ctl, s);
+  return pair ? launch_rk<RK, true, false>(p, in, out, stats, ctl, s) : launch_rk<RK, false, false>(p, in, out, stats, ctl, s);
+}
+
 // pair: evaluate the x- and y-face of a row together (one vote for both);
-// otherwise one after the other.
+// otherwise one after the other.  stage: paired faces, rows staged through
+// shared memory (march_strip_staged).
 inline cudaError_t launch(const EcgFvParams& p, const double* in, double* out, EcgStepStats* stats,
-                          const EcgDtCtl& ctl, cudaStream_t s, bool pair)
+                          const EcgDtCtl& ctl, cudaStream_t s, bool pair, bool stage)
 {
   switch (p.riemann) {
-    case ECG_RIEMANN_RUSANOV:
-      return pair ? launch_rk<ECG_RIEMANN_RUSANOV, true>(p, in, out, stats, ctl, s)
-                  : launch_rk<ECG_RIEMANN_RUSANOV, false>(p, in, out, stats, ctl, s);
-    case ECG_RIEMANN_LOWMACH_HLLC:
-      return pair ? launch_rk<ECG_RIEMANN_LOWMACH_HLLC, true>(p, in, out, stats, ctl, s)
-                  : launch_rk<ECG_RIEMANN_LOWMACH_HLLC, false>(p, in, out, stats, ctl, s);
+    case ECG_RIEMANN_RUSANOV: return launch_mode<ECG_RIEMANN_RUSANOV>(p, in, out, stats, ctl, s, pair, stage);
+    case ECG_RIEMANN_LOWMACH_HLLC: return launch_mode<ECG_RIEMANN_LOWMACH_HLLC>(p, in, out, stats, ctl, s, pair, stage);
     case ECG_RIEMANN_XIE_AM_HLLC_P: return fast::launch(p, in, out, stats, ctl, s);  // needs the 5-face sensor
-    default:
-      return pair ? launch_rk<ECG_RIEMANN_HLLC, true>(p, in, out, stats, ctl, s)
-                  : launch_rk<ECG_RIEMANN_HLLC, false>(p, in, out, stats, ctl, s);
+    default: return launch_mode<ECG_RIEMANN_HLLC>(p, in, out, stats, ctl, s, pair, stage);
   }
 }
 

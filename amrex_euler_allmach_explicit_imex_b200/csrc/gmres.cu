@@ -53,7 +53,8 @@ constexpr int kMinCycle = 16;  // mixed: shortest cycle a restart may end
 
 struct GridBar {
   unsigned int arrive;  // arrivals; the top bit is the timeout flag
-  unsigned int pad[3];
+  unsigned int settle;  // deterministic mode: blocks that have written their partial sums
+  unsigned int pad[2];
 };
 
 struct GmresArgs {
@@ -68,6 +69,7 @@ struct GmresArgs {
   float* V32;    // (m+1) x n (mixed)
   double* part;  // residual_kernel: 2 x its blocks
   double* acc;   // three accumulator rows of ld doubles, zeroed by the host before the launch
+  double* dpt;   // deterministic mode: three tables of per-block partial sums (nblocks x ld each)
   double* R;     // column-major (m+1) x m
   GridBar* bar;
   EcgGmresResult* res;
@@ -82,6 +84,7 @@ struct GmresArgs {
   int reorth;         // mixed: DGKS test of the FP32-basis cycles, 1 as the FP64 solve, 0 severe cancellation only
   int kres;           // basis vectors resident in shared memory on each block's rows
   int prow;           // rows of a block (the last may have fewer)
+  int det;            // grid sums in a fixed order (bit-reproducible solves)
   long long spin_limit;
 };
 
@@ -346,6 +349,7 @@ struct Smem {
   double* scratch;
   double* vs;  // resident basis vectors (TV)
   double* dpart;
+  double* cnt;  // block 0: vector accesses per row of the solve, [0] FP64 vectors, [1] basis vectors stored as FP32
 };
 __device__ __forceinline__ Smem carve(double* base, int m)
 {
@@ -359,14 +363,29 @@ __device__ __forceinline__ Smem carve(double* base, int m)
   s.coef = s.red + L;
   s.wpart = s.coef + L;
   s.scratch = s.wpart + NW;
-  s.dpart = s.scratch + NT + L;
+  s.cnt = s.scratch + NT + L;
+  s.dpart = s.cnt + 2;
   s.vs = s.dpart + NW * dots_ld(m);
   return s;
 }
 // bytes of the fixed part; the resident basis vectors follow it
 inline size_t smem_bytes(int m)
 {
-  return sizeof(double) * (static_cast<size_t>(7) * (m + 8) + NW + NT + static_cast<size_t>(NW) * dots_ld(m));
+  return sizeof(double) * (static_cast<size_t>(7) * (m + 8) + NW + NT + 2 + static_cast<size_t>(NW) * dots_ld(m));
+}
+
+// Algorithmic traffic of the solve, counted by block 0's thread 0 in
+// vector-element accesses per row: a sweep that reads or writes one vector of
+// n entries counts 1 (the operator's 9-point stencil reads its input vector
+// once, and the two face-enthalpy arrays as one vector each).  nb: accesses to
+// basis vectors (FP64 or FP32, the TV of the solve), n64: to FP64 vectors.
+template <typename TV>
+__device__ __forceinline__ void count(const Smem& S, double n64, double nb)
+{
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S.cnt[0] += n64 + (sizeof(TV) == 8 ? nb : 0.0);
+    S.cnt[1] += sizeof(TV) == 8 ? 0.0 : nb;
+  }
 }
 
 // Per-thread value v of one sum -> per-warp partial (lane 0 stores).
@@ -385,19 +404,73 @@ __device__ __forceinline__ void warp_partial(double v, double* wpart)
 // after reading row k, block 0 clears row k + 2, which no block reads or
 // writes again before the barrier that precedes the producers of reduction
 // k + 2.
+//
+// Deterministic mode (dpt set): a block writes its partial sums of reduction
+// k into its own slot of partial table k % 3 instead, and the block that
+// writes its partials last adds them up in block order into the row before
+// the grid barrier (acc_settle), so every launch on the same inputs gives the
+// same bits.  Maxima are exact in any order and stay atomic.
 struct Acc {
   double* rows;
   int ld;
+  double* dpt;  // per-block partial tables (deterministic mode), else null
   __device__ __forceinline__ double* row(unsigned int k) const { return rows + (k % 3) * ld; }
 };
 
-__device__ __forceinline__ void acc_add(double* row, int q, double v) { atomicAdd(row + q, v); }
+// Destination of one block's partial sums of one reduction.
+struct SumSink {
+  double* p;
+  bool det;
+};
+__device__ __forceinline__ SumSink sink(const Acc& A, unsigned int k)
+{
+  if (A.dpt) return SumSink{A.dpt + (static_cast<size_t>(k % 3) * gridDim.x + blockIdx.x) * A.ld, true};
+  return SumSink{A.row(k), false};
+}
+
+__device__ __forceinline__ void acc_add(const SumSink& s, int q, double v)
+{
+  if (s.det) s.p[q] = v;
+  else atomicAdd(s.p + q, v);
+}
 
 // Maxima are nonnegative or NaN (with the sign bit clear), which order as
 // their bit patterns, NaN above every number.
 __device__ __forceinline__ void acc_max(double* row, int q, double v)
 {
   atomicMax(reinterpret_cast<unsigned long long*>(row + q), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+// Deterministic mode, after every block has written its partial sums of
+// reduction k (entries [0, ns)) and before the grid barrier that precedes
+// their readers: the block that arrives last sums the partial table in block
+// order (lane l takes blocks l, l + 32, ..., then a fixed shuffle tree) into
+// row k.  The arrival count only grows; nset counts the settles passed.
+__device__ __forceinline__ void acc_settle(const Acc& A, GridBar* bar, unsigned int k, int ns, unsigned int& nset)
+{
+  if (!A.dpt) return;
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int v = atomicAdd(&bar->settle, 1u);
+    last = v + 1u == (nset + 1u) * gridDim.x ? 1 : 0;
+  }
+  ++nset;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double* tab = A.dpt + static_cast<size_t>(k % 3) * gridDim.x * A.ld;
+  double* row = A.row(k);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = warp; q < ns; q += NW) {
+    double s = 0.0;
+    for (int b = lane; b < static_cast<int>(gridDim.x); b += 32) s += __ldcg(tab + static_cast<size_t>(b) * A.ld + q);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) __stcg(row + q, s);
+  }
+  __syncthreads();
 }
 
 // After the grid barrier that follows the producers of reduction k: out[q] =
@@ -415,8 +488,8 @@ __device__ __forceinline__ void acc_read(const Acc& A, unsigned int& k, int ne, 
 }
 
 // Adds the sum of the warp partials, in warp order, to entry q of an
-// accumulator row.
-__device__ __forceinline__ void commit_sum(const double* wpart, double* row, int q)
+// accumulator row (or writes it to the block's partial slot).
+__device__ __forceinline__ void commit_sum(const double* wpart, const SumSink& row, int q)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -516,7 +589,7 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&s)[DG], int lane)
 // the warps' partials summed in warp order.
 template <typename TV>
 __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __restrict__ w, Rows rw, int nvec,
-                                           bool with_norm, double* row, double* dpart, bool pair)
+                                           bool with_norm, const SumSink& row, double* dpart, bool pair)
 {
   const TV* __restrict__ V = bs.V;
   const long long n = bs.n;
@@ -760,7 +833,7 @@ template <typename TV, bool RES>
 __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec, const double* x0vec, double* xvec,
                              TV* __restrict__ V, double* __restrict__ w,
                              double* __restrict__ rres, int kmax, double tol, double restart_rtol, unsigned int& gen,
-                             unsigned int& nred, double* shbase)
+                             unsigned int& nred, unsigned int& nset, double* shbase)
 {
   const long long n = a.n;
   const Rows rw = own_rows(n);
@@ -771,6 +844,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   // RES = false: no resident vectors (K a constant 0, the shared-memory
   // paths compiled out, the register budget of the plain solve)
   const Basis<TV> bs{V, n, reinterpret_cast<TV*>(S.vs), RES ? a.kres : 0, a.prow, rw.r0};
+  const Acc A{a.acc, a.ld, a.det ? a.dpt : nullptr};
   SolveState st;
   st.it = 0;
   st.best_it = 0;
@@ -786,19 +860,21 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     if (wide) sweep_r0<2>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
     else sweep_r0<1>(a.op, rw, bvec, x0vec, w, rres, bmax, rmax, r2);
     warp_partial(r2, S.wpart);
-    commit_sum(S.wpart, Acc{a.acc, a.ld}.row(nred), 0);
+    commit_sum(S.wpart, sink(A, nred), 0);
     bmax = block_max(bmax, S.scratch);
     rmax = block_max(rmax, S.scratch);
     if (threadIdx.x == 0) {
-      acc_max(Acc{a.acc, a.ld}.row(nred), 1, bmax);
-      acc_max(Acc{a.acc, a.ld}.row(nred), 2, rmax);
+      acc_max(A.row(nred), 1, bmax);
+      acc_max(A.row(nred), 2, rmax);
     }
+    acc_settle(A, a.bar, nred, 1, nset);
   }
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
     st.timeout = 1;
     return st;
   }
-  acc_read(Acc{a.acc, a.ld}, nred, 3, S.red);
+  acc_read(A, nred, 3, S.red);
+  count<TV>(S, 6.0, 0.0);  // r0 = b - A x0: x0, hx, hy, b read; w, rres written
   beta = sqrt(S.red[0]);
   const double bn_raw = S.red[1];
   const double r0inf = S.red[2];
@@ -869,7 +945,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     if (broke || j >= kmax) {
       // no further column: the test of iterate j on its own
       if (j > 0) {
-        acc_read(Acc{a.acc, a.ld}, nred, j + 4, S.red);
+        acc_read(A, nred, j + 4, S.red);
         if (check(j, S.red[j + 3])) break;
       }
       if (broke) st.breakdown = 1;
@@ -879,7 +955,9 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     // ---- sweep A: w = A v_j; d_i = v_i . w (i <= j); ||w||^2; nonfinite ----
     if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
     else sweep_spmv<TV, 1>(a.op, rw, vj, w);
-    block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart, pair);
+    block_dots<TV>(bs, w, rw, j + 1, true, sink(A, nred), S.dpart, pair);
+    count<TV>(S, 4.0, j + 2.0);  // w = A v_j (v_j, hx, hy, w); v_i . w (j + 1 vectors, w)
+    acc_settle(A, a.bar, nred, j + 3, nset);
     if (!grid_sync(a.bar, gen, a.spin_limit)) {
       st.timeout = 1;
       return st;
@@ -887,7 +965,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     // the dot products and, in the same read, the residual maximum of iterate
     // j: the test runs here, one sweep A later than its data, so it costs no
     // reduction of its own (a stopping iterate discards this w)
-    acc_read(Acc{a.acc, a.ld}, nred, j > 0 ? j + 4 : j + 3, S.red);
+    acc_read(A, nred, j > 0 ? j + 4 : j + 3, S.red);
     if (j > 0 && check(j, S.red[j + 3])) break;
     if (S.red[j + 2] != 0.0) {
       st.nonfinite = 1;
@@ -910,12 +988,14 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
       if (wide) sweep_combine<TV, true, 2>(rw, bs, S.coef, j + 1, w, w);
       else sweep_combine<TV, true, 1>(rw, bs, S.coef, j + 1, w, w);
-      block_dots<TV>(bs, w, rw, j + 1, true, Acc{a.acc, a.ld}.row(nred), S.dpart, pair);
+      block_dots<TV>(bs, w, rw, j + 1, true, sink(A, nred), S.dpart, pair);
+      count<TV>(S, 3.0, 2.0 * (j + 1));  // w -= V d (j + 1 vectors, w twice); v_i . w again
+      acc_settle(A, a.bar, nred, j + 3, nset);
       if (!grid_sync(a.bar, gen, a.spin_limit)) {
         st.timeout = 1;
         return st;
       }
-      acc_read(Acc{a.acc, a.ld}, nred, j + 2, S.red);
+      acc_read(A, nred, j + 2, S.red);
       sw = S.red[j + 1];
       nn2 = sw - sum_squares(S.red, j + 1);
       for (int q = threadIdx.x; q <= j; q += NT) {
@@ -1011,8 +1091,9 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
       }
     }
     st.it = j + 1;
+    count<TV>(S, 3.0, j + 2.0);  // v_{j+1} = (w - V coef) / nn: j + 1 vectors, w, v_{j+1}; rres read and written
     rmx = block_max(rmx, S.scratch);
-    if (threadIdx.x == 0) acc_max(Acc{a.acc, a.ld}.row(nred), j + 4, rmx);  // entry (j+1)+3, read after the next sweep A
+    if (threadIdx.x == 0) acc_max(A.row(nred), j + 4, rmx);  // entry (j+1)+3, read after the next sweep A
   }
   // ---- x = x0 + V_k y_k for the returned iterate k ----
   if (!grid_sync(a.bar, gen, a.spin_limit)) {
@@ -1030,6 +1111,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
   if (ynf) k = 0;  // x = x0
   if (wide) sweep_combine<TV, false, 2>(rw, bs, y, k, x0vec, xvec);
   else sweep_combine<TV, false, 1>(rw, bs, y, k, x0vec, xvec);
+  count<TV>(S, 2.0, k);  // x = x0 + V_k y: x0, x, k vectors
   return st;
 }
 
@@ -1041,12 +1123,17 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   extern __shared__ double sh[];
   unsigned int gen = 0;   // barriers passed; the counter is zeroed by the host before the launch
   unsigned int nred = 0;  // accumulator reductions completed
+  unsigned int nset = 0;  // deterministic mode: partial-sum settles passed
   EcgGmresResult out;
   std::memset(&out, 0, sizeof(out));
   const int limit = a.max_iter < a.n ? a.max_iter : static_cast<int>(a.n);
+  {
+    const Smem S0 = carve(sh, a.m);
+    if (threadIdx.x == 0) S0.cnt[0] = S0.cnt[1] = 0.0;
+  }
   if constexpr (!MIXED) {
     const SolveState st =
-        krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, nred, sh);
+        krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, nred, nset, sh);
     out.iterations = st.best_it;
     out.converged = st.converged;
     out.breakdown = st.breakdown;
@@ -1069,7 +1156,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
       const bool last = cycles + 1 >= a.max_refine;
       const int kin = per_cycle < left ? per_cycle : left;
       st = krylov<float, RES>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol, gen,
-                              nred, sh);
+                              nred, nset, sh);
       if (cycles == 0) {
         out.initial_linf = st.r0_linf;
         out.b_linf = st.b_linf;
@@ -1102,7 +1189,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   if (!out.timeout && grid_sync(a.bar, gen, a.spin_limit)) {
     const Rows rw = own_rows(a.n);
     const Smem S = carve(sh, a.m);
-    const Acc A{a.acc, a.ld};
+    const Acc A{a.acc, a.ld, nullptr};  // maxima only
     double rmax = 0.0, bmax = 0.0;
     for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += NT) {
       const int qq[1] = {q};
@@ -1129,7 +1216,12 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   } else {
     out.timeout = 1;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *a.res = out;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const Smem S = carve(sh, a.m);
+    out.vec_access64 = S.cnt[0] + 4.0;  // the final residual: x, hx, hy, b
+    out.vec_access32 = S.cnt[1];
+    *a.res = out;
+  }
 }
 
 // ---- residual A x - b (FP64), ||.||inf, max(||b||inf, 1), nonfinite -------------------
@@ -1198,6 +1290,7 @@ struct EcgGmresWork {
   float* V32 = nullptr;
   double* part = nullptr;  // residual_kernel's block maxima
   double* acc = nullptr;   // three accumulator rows of ld doubles
+  double* dpt = nullptr;   // deterministic mode: three per-block partial tables (nblocks x ld)
   int ld = 0;
   double* R = nullptr;
   GridBar* bar = nullptr;
@@ -1261,6 +1354,7 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   alloc(reinterpret_cast<void**>(&w->r), sizeof(double) * n);
   alloc(reinterpret_cast<void**>(&w->part), sizeof(double) * 2 * kResidualBlocks);
   alloc(reinterpret_cast<void**>(&w->acc), sizeof(double) * 3 * w->ld);
+  alloc(reinterpret_cast<void**>(&w->dpt), sizeof(double) * 3 * static_cast<size_t>(w->nblocks) * w->ld);
   alloc(reinterpret_cast<void**>(&w->R), sizeof(double) * (w->m + 1) * (w->m + 1));
   alloc(reinterpret_cast<void**>(&w->bar), sizeof(GridBar));
   alloc(reinterpret_cast<void**>(&w->d_res), sizeof(EcgGmresResult));
@@ -1297,6 +1391,7 @@ void gmres_work_destroy(EcgGmresWork* w)
   cudaFree(w->V32);
   cudaFree(w->part);
   cudaFree(w->acc);
+  cudaFree(w->dpt);
   cudaFree(w->R);
   cudaFree(w->bar);
   cudaFree(w->d_res);
@@ -1307,7 +1402,7 @@ void gmres_work_destroy(EcgGmresWork* w)
 
 cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
                         int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
-                        int reorth, EcgGmresResult* out, cudaStream_t s)
+                        int reorth, bool det, EcgGmresResult* out, cudaStream_t s)
 {
   if (mixed != w->mixed) return cudaErrorInvalidValue;  // the basis is allocated for one precision
   GmresArgs a;
@@ -1323,6 +1418,8 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.V32 = w->V32;
   a.part = w->part;
   a.acc = w->acc;
+  a.dpt = w->dpt;
+  a.det = det ? 1 : 0;
   a.R = w->R;
   a.bar = w->bar;
   a.res = w->d_res;

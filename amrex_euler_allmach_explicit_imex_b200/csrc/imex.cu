@@ -275,7 +275,7 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     EcgGmresResult g;
     if (!ecgi::cuda_ok(c, gmres_solve(im->gw, op, im->rhs, im->p, im->x, c->cfg.imex_solver_max_iter, tol, mixed,
                                       c->opt.mixed_inner_max_iter, c->opt.mixed_inner_rtol,
-                                      c->opt.mixed_max_refinements, c->opt.mixed_reorth, &g, s),
+                                      c->opt.mixed_max_refinements, c->opt.mixed_reorth, c->opt.deterministic != 0, &g, s),
                        "gmres"))
       return ECG_ERR_CUDA;
     if (g.timeout) {
@@ -290,6 +290,7 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     d.solver_iterations += g.iterations;
     d.gmres_inner_iterations += g.inner_iterations;
     d.gmres_refinements += g.refinements;
+    d.gmres_vector_bytes += static_cast<double>(n) * (8.0 * g.vec_access64 + 4.0 * g.vec_access32);
     const int nf = std::isfinite(g.final_linf) && std::isfinite(g.final_b_linf) ? 0 : 1;
     const double lr = nf ? nan : g.final_linf;
     d.pressure_linear_residual_linf = lr;

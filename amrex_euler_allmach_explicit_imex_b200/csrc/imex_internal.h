@@ -100,6 +100,10 @@ struct EcgGmresResult {
   // ||b||inf at the start, ||A x - b||inf and ||b||inf of the returned x
   // (NaN when nonfinite; the final pair is NaN after a timeout)
   double initial_linf, b_linf, final_linf, final_b_linf;
+  // algorithmic traffic: vector-element accesses per row of the whole solve
+  // (one sweep over one vector counts 1), to FP64 vectors and to FP32 basis
+  // vectors; bytes = n (8 vec_access64 + 4 vec_access32)
+  double vec_access64, vec_access32;
 };
 
 struct EcgGmresWork;  // gmres.cu
@@ -108,10 +112,12 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
 void gmres_work_destroy(EcgGmresWork* w);
 // Solves A x = b from x0 (device vectors of n doubles) with the reference's
 // semantics (solve_host_sparse_gmres, imex/imex_pressure_helpers.hpp:92-217).
-// mixed: FP32 inner GMRES inside FP64 iterative refinement.
+// mixed: cycles on an FP32-stored Krylov basis, each opened with the true
+// FP64 residual.  det: grid sums in a fixed block order, so repeated solves of
+// the same system give the same bits.
 cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
                         int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
-                        int reorth, EcgGmresResult* out, cudaStream_t s);
+                        int reorth, bool det, EcgGmresResult* out, cudaStream_t s);
 // r = A x - b: infinity norm, rhs infinity norm (max(|b|inf, 1)) and nonfinite flag.
 cudaError_t pressure_residual(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x,
                               double* res_linf, double* rhs_norm, int* nonfinite, cudaStream_t s);

@@ -21,11 +21,15 @@
 // other's statistics and ring.
 //
 // The first call on each device looks up the array's address with
-// cudaGetSymbolAddress (with that device current) and checks that the device
-// is a compute-capability 10 part; the first call should therefore come
-// before any stream capture.
+// cudaGetSymbolAddress (with that device current), reads the device's SM count
+// and checks that the device is a compute-capability 10 part; the first call
+// should therefore come before any stream capture.  The address is kept until
+// the process exits: a cudaDeviceReset (or any teardown of the device's primary
+// context) leaves it pointing into a context that no longer exists, so callers
+// that reset a device must not call this entry point on it afterwards.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -48,6 +52,7 @@ __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_addr[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};  // SM count of each device, read with its address
 
 void set_err(char* err, int32_t len, const char* msg)
 {
@@ -55,8 +60,9 @@ void set_err(char* err, int32_t len, const char* msg)
   std::snprintf(err, static_cast<size_t>(len), "%s", msg);
 }
 
-// Address of g_scratch on `dev` (current); looked up once per device.
-ecg_status scratch_on(int dev, unsigned char** out, char* err, int32_t len)
+// Address of g_scratch on `dev` (current) and the device's SM count; looked
+// up once per device.
+ecg_status scratch_on(int dev, unsigned char** out, int* sms, char* err, int32_t len)
 {
   if (dev < 0 || dev >= kMaxDevices) {
     set_err(err, len, "device ordinal out of range");
@@ -69,6 +75,11 @@ ecg_status scratch_on(int dev, unsigned char** out, char* err, int32_t len)
       set_err(err, len, "device is not a compute-capability 10 (B200-class) GPU");
       return ECG_ERR_NO_DEVICE;
     }
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) {
+      set_err(err, len, "device SM count unavailable");
+      return ECG_ERR_CUDA;
+    }
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess || !p) {
@@ -78,8 +89,10 @@ ecg_status scratch_on(int dev, unsigned char** out, char* err, int32_t len)
       return ECG_ERR_CUDA;
     }
     g_addr[dev] = static_cast<unsigned char*>(p);
+    g_sms[dev] = nsm;
   }
   *out = g_addr[dev];
+  *sms = g_sms[dev];
   return ECG_OK;
 }
 
@@ -139,6 +152,17 @@ ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gp
     set_err(err, err_len, "layout does not cover [0, nx) x [0, ny)");
     return ECG_ERR_BAD_ARG;
   }
+  // The step reads neighbour cells of state_in while it writes state_out, so
+  // the two arrays (4 planes of nstride doubles from their Array4 bases) must
+  // not share a byte.
+  {
+    const auto a0 = reinterpret_cast<uintptr_t>(state_in), b0 = reinterpret_cast<uintptr_t>(state_out);
+    const uintptr_t len = sizeof(double) * 4 * static_cast<uintptr_t>(nstride);
+    if (a0 < b0 + len && b0 < a0 + len) {
+      set_err(err, err_len, "state_in and state_out overlap");
+      return ECG_ERR_BAD_ARG;
+    }
+  }
   ecg_gpu_options o;
   if (opt) o = *opt;
   else ecg_default_gpu_options(&o);
@@ -162,11 +186,12 @@ ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gp
   cudaError_t e = guard.enter(o.device);
   if (e != cudaSuccess) return fail(err, err_len, ECG_ERR_NO_DEVICE, "select device", e);
   unsigned char* scratch = nullptr;
-  const ecg_status st = scratch_on(o.device, &scratch, err, err_len);
+  int sms = 0;
+  const ecg_status st = scratch_on(o.device, &scratch, &sms, err, err_len);
   if (st != ECG_OK) return st;
 
   const EcgStencilOps* ops = o.arith == ECG_ARITH_EXACT ? &ecg_exact_ops : &ecg_fast_ops;
-  const int tile_y = (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
+  const int tile_y = (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 3 || o.tile_y == 8 || o.tile_y == 16) ? o.tile_y : 0;
   cudaStream_t s = static_cast<cudaStream_t>(o.stream);
 
   // grid of ecg_create with the caller's strides
@@ -185,6 +210,7 @@ ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gp
   p.limiter = cfg->slope_limiter;
   p.riemann = cfg->riemann;
   p.march_rows = o.tile_x;
+  p.sm_count = sms;
   const int64_t off = static_cast<int64_t>(-lo_x) + static_cast<int64_t>(-lo_y) * jstride;
   const double* u = state_in + off;
   double* v = state_out + off;

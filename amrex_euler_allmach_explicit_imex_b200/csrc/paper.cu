@@ -649,7 +649,8 @@ extern "C" ecg_status ecg_paper_t1s2_run(ecg_ctx* c, const ecg_paper_options* op
       ecg_paper::rhs_kernel<<<blocks(n), NT, 0, s>>>(C, B.star, B.corr, B.hx, B.hy, dt, t1, cx, cy, B.rhs, B.acc);
       if (!ecgi::cuda_ok(c, cudaGetLastError(), "paper rows")) return ECG_ERR_CUDA;
       EcgGmresResult g;
-      if (!ecgi::cuda_ok(c, gmres_solve(B.gw, op, B.rhs, B.p, B.x, max_iter, cfg.imex_solver_tol, false, 0, 0.0, 0, 1, &g, s),
+      if (!ecgi::cuda_ok(c, gmres_solve(B.gw, op, B.rhs, B.p, B.x, max_iter, cfg.imex_solver_tol, false, 0, 0.0, 0, 1,
+                                            c->opt.deterministic != 0, &g, s),
                          "gmres"))
         return ECG_ERR_CUDA;
       if (g.timeout) {

@@ -28,43 +28,46 @@ __device__ __forceinline__ int wrapi(int i, int n)
   return r < 0 ? r + n : r;
 }
 
-// Conserved state of cell (i, j), i or j possibly outside the domain.  The
-// index map reproduces the ghost values that fill_problem_ghosts writes
-// (boundary_conditions.hpp:2-73): periodic wrap, outflow clamp, bubble wall
-// mirror (row -j-1, my negated) and bubble inflow state; exact-state
+// Where the conserved state of cell (i, j) comes from, i or j possibly
+// outside the domain: the four component planes at p, p + pl, p + 2 pl,
+// p + 3 pl (with my negated when flip), or the constant state bc.cst when p is
+// null.  The index map reproduces the ghost values that fill_problem_ghosts
+// writes (boundary_conditions.hpp:2-73): periodic wrap, outflow clamp, bubble
+// wall mirror (row -j-1, my negated) and bubble inflow state; exact-state
 // Dirichlet kinds read the precomputed ghost ring.
-__device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __restrict__ u, int i, int j)
+struct CellSrc {
+  const double* p;
+  long long pl;
+  bool flip;
+};
+
+__device__ __forceinline__ CellSrc cell_src(const EcgFvParams& P, const double* __restrict__ u, int i, int j)
 {
   const int nx = P.g.nx, ny = P.g.ny;
-  if (static_cast<unsigned>(i) < static_cast<unsigned>(nx) && static_cast<unsigned>(j) < static_cast<unsigned>(ny)) {
-    const long long o = static_cast<long long>(j) * P.g.pitch + i;
-    const long long pl = P.g.plane;
-    return Cons{__ldg(u + o), __ldg(u + o + pl), __ldg(u + o + 2 * pl), __ldg(u + o + 3 * pl)};
-  }
+  if (static_cast<unsigned>(i) < static_cast<unsigned>(nx) && static_cast<unsigned>(j) < static_cast<unsigned>(ny))
+    return CellSrc{u + static_cast<long long>(j) * P.g.pitch + i, P.g.plane, false};
   if (P.bc.ring) {
     // Tiles and warp strips that overhang the domain load cells past the
     // two-cell ring; their values feed no in-domain face, so clamp them onto
     // the ring to keep every read inside it.
     i = i < -2 ? -2 : (i > nx + 1 ? nx + 1 : i);
     j = j < -2 ? -2 : (j > ny + 1 ? ny + 1 : j);
-    const long long o = static_cast<long long>(j + 2) * P.ring_pitch + (i + 2);
-    const long long pl = P.ring_plane;
-    return Cons{P.ring[o], P.ring[o + pl], P.ring[o + 2 * pl], P.ring[o + 3 * pl]};
+    return CellSrc{P.ring + static_cast<long long>(j + 2) * P.ring_pitch + (i + 2), P.ring_plane, false};
   }
   int hs = -1;  // halo column of a slab side: 0, 1 left (x = -2, -1), 2, 3 right (x = nx, nx + 1)
   if (i < 0) {
     if (P.bc.x_lo == BC_HALO) hs = i < -2 ? 0 : i + 2;
-    else if (P.bc.x_lo == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+    else if (P.bc.x_lo == BC_CONST) return CellSrc{nullptr, 0, false};
     else i = P.bc.x_lo == BC_PERIODIC ? wrapi(i, nx) : 0;
   } else if (i >= nx) {
     // strips past the last column read cells beyond the halo; they feed no face of the slab
     if (P.bc.x_hi == BC_HALO) hs = i - nx > 1 ? 3 : 2 + (i - nx);
-    else if (P.bc.x_hi == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+    else if (P.bc.x_hi == BC_CONST) return CellSrc{nullptr, 0, false};
     else i = P.bc.x_hi == BC_PERIODIC ? wrapi(i, nx) : nx - 1;
   }
   bool flip = false;
   if (j < 0) {
-    if (P.bc.y_lo == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+    if (P.bc.y_lo == BC_CONST) return CellSrc{nullptr, 0, false};
     if (P.bc.y_lo == BC_PERIODIC) {
       j = wrapi(j, ny);
     } else if (P.bc.y_lo == BC_REFLECT) {
@@ -75,7 +78,7 @@ __device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __
       j = 0;
     }
   } else if (j >= ny) {
-    if (P.bc.y_hi == BC_CONST) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+    if (P.bc.y_hi == BC_CONST) return CellSrc{nullptr, 0, false};
     if (P.bc.y_hi == BC_PERIODIC) {
       j = wrapi(j, ny);
     } else if (P.bc.y_hi == BC_REFLECT) {
@@ -90,16 +93,20 @@ __device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __
     // the neighbour slab's cell, after the y policy (a corner ghost is the
     // y-mapped row of the halo column, as in the undivided grid)
     const long long fs = 2LL * ny;
-    const double* h = (hs < 2 ? P.halo_lo : P.halo_hi) + static_cast<long long>(j) * 2 + (hs & 1);
-    Cons c{h[0], h[fs], h[2 * fs], h[3 * fs]};
-    if (flip) c.my = -c.my;
-    return c;
+    return CellSrc{(hs < 2 ? P.halo_lo : P.halo_hi) + static_cast<long long>(j) * 2 + (hs & 1), fs, flip};
   }
-  const long long o = static_cast<long long>(j) * P.g.pitch + i;
-  const long long pl = P.g.plane;
-  Cons c{__ldg(u + o), __ldg(u + o + pl), __ldg(u + o + 2 * pl), __ldg(u + o + 3 * pl)};
-  if (flip) c.my = -c.my;
-  return c;
+  return CellSrc{u + static_cast<long long>(j) * P.g.pitch + i, P.g.plane, flip};
+}
+
+// Conserved state of cell (i, j), i or j possibly outside the domain
+// (cell_src's ghost policy).
+__device__ __forceinline__ Cons load_cell(const EcgFvParams& P, const double* __restrict__ u, int i, int j)
+{
+  const CellSrc c = cell_src(P, u, i, j);
+  if (!c.p) return Cons{P.bc.cst[0], P.bc.cst[1], P.bc.cst[2], P.bc.cst[3]};
+  Cons r{__ldg(c.p), __ldg(c.p + c.pl), __ldg(c.p + 2 * c.pl), __ldg(c.p + 3 * c.pl)};
+  if (c.flip) r.my = -r.my;
+  return r;
 }
 
 // ---- block reductions --------------------------------------------------------
@@ -481,10 +488,13 @@ cudaError_t launch_fv_step(const EcgFvParams& p, const double* in, double* out, 
                            const EcgDtCtl& ctl, int tile_y, cudaStream_t s)
 {
 #ifdef ECG_FAST_KERNEL
-  // 0: column-strip kernel, x- and y-faces evaluated together (default);
-  // 2: column-strip kernel, faces one after the other; 1: square-tile kernel
-  if (tile_y == 0) return march::launch(p, in, out, stats, ctl, s, true);
-  if (tile_y == 2) return march::launch(p, in, out, stats, ctl, s, false);
+  // 0: column-strip kernel, x- and y-faces evaluated together, rows staged
+  // through shared memory (default); 3: the same with rows loaded straight
+  // into registers; 2: column-strip kernel, faces one after the other, rows
+  // into registers; 1: square-tile kernel
+  if (tile_y == 0) return march::launch(p, in, out, stats, ctl, s, true, true);
+  if (tile_y == 3) return march::launch(p, in, out, stats, ctl, s, true, false);
+  if (tile_y == 2) return march::launch(p, in, out, stats, ctl, s, false, false);
   if (tile_y == 1) return fast::launch(p, in, out, stats, ctl, s);
 #endif
   switch (p.riemann) {

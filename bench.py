@@ -304,31 +304,46 @@ def mach122_imex_kv(nx, ny):
 
 
 IMEX_CASES = [("gresho_vortex 256x256 periodic, M=0.01", imex_kv(256, 0.01)),
+              ("gresho_vortex 256x256 periodic, M=0.1", imex_kv(256, 0.1)),
+              ("gresho_vortex 256x256 periodic, M=0.001", imex_kv(256, 0.001)),
               ("gresho_vortex 768x768 periodic, M=0.01", imex_kv(768, 0.01)),
+              ("shock_density_bubble_2d 640x160", bubble_imex_kv(640, 160)),
               ("shock_density_bubble_2d 2560x640", bubble_imex_kv(2560, 640)),
               ("shock_bubble_mach122 2560x640 on [0,4]x[0,1]", mach122_imex_kv(2560, 640))]
+
+# Algorithmic bytes of an IMEX step outside GMRES, per cell: the star update
+# (read U, write U*, p, K: 88 B), per Picard pass the assembly (80 B: U*, p,
+# K read, face enthalpies and rhs written) and the p / eq54 momentum refresh
+# (56 B: x read, p written; m*, p read, K written), and the closeout (48 B).
+# The GMRES sweeps' bytes come from the solve's own count of the vector
+# sweeps it ran (ecg_imex_diag.gmres_vector_bytes).
+IMEX_STAR_B, IMEX_PICARD_B, IMEX_CLOSE_B = 88, 80 + 56, 48
 
 
 def imex_leg(dev, stream, steps=3):
     """Each IMEX_CASES configuration, IMEX T1/S2 (4 Picard solves, GMRES tol
     1e-10): time per step of the all-FP64 solve and of the FP32-basis /
-    FP64-arithmetic solve on the same GPU, their GMRES iterations, and the
-    relative drift between their states after `steps` + 1 steps."""
+    FP64-arithmetic solve on the same GPU, their GMRES iterations and solver
+    statuses, the step's algorithmic bytes and HBM fraction, and the drift
+    between the two states after `steps` + 1 steps (max-norm relative, and the
+    relative difference of the density in L1)."""
     import torch
 
     from amrex_euler_allmach_explicit_imex_b200 import api
     from amrex_euler_allmach_explicit_imex_b200.config import read_config
 
+    peak, _ = peaks()
     cases = []
     for name, kv in IMEX_CASES:
         cfg = read_config(kv).cfg
+        cells = cfg.n_cell[0] * cfg.n_cell[1]
         out = {}
         states = {}
         for prec in ("fp64", "mixed"):
             with api.Context(cfg, imex_precision=prec, device=dev.index or 0, stream=stream.cuda_stream) as ctx:
                 api.initialize_state(ctx)
                 t = 0.0
-                ms, its, statuses = [], [], []
+                ms, its, statuses, gbytes = [], [], [], []
                 for k in range(steps + 1):
                     dt, _ = api.compute_imex_dt(ctx, t)
                     a = torch.cuda.Event(enable_timing=True)
@@ -341,41 +356,113 @@ def imex_leg(dev, stream, steps=3):
                     if k > 0:
                         ms.append(a.elapsed_time(b))
                         its.append(d.gmres_inner_iterations if prec == "mixed" else d.solver_iterations)
+                        gbytes.append(d.gmres_vector_bytes)
                     t += dt
                 states[prec] = ctx.download()
-                out[prec] = {"ms_per_step": statistics.median(ms), "gmres_iterations": its,
-                             "status": api.solver_status_str(d.solver_status), "step_statuses": statuses}
-        drift = float(np.abs(states["fp64"] - states["mixed"]).max() / np.abs(states["fp64"]).max())
+                med = statistics.median(ms)
+                gb = statistics.median(gbytes)
+                other = cells * (IMEX_STAR_B + cfg.imex_picard_iterations * IMEX_PICARD_B + IMEX_CLOSE_B)
+                step_bytes = gb + other
+                out[prec] = {"ms_per_step": med, "gmres_iterations": its, "status": statuses[-1],
+                             "step_statuses": statuses, "gmres_bytes_per_step": gb, "step_bytes": step_bytes,
+                             "achieved_gbs": step_bytes / (med * 1e-3) / 1e9,
+                             "hbm_frac": step_bytes / (med * 1e-3) / 1e9 / peak}
+        f, m = states["fp64"], states["mixed"]
+        drift = float(np.abs(f - m).max() / np.abs(f).max())
+        l1drift = float(np.abs(f[0] - m[0]).sum() / np.abs(f[0]).sum())
+        ok = all(x.startswith("converged") for p in ("fp64", "mixed") for x in out[p]["step_statuses"])
         cases.append({"workload": name + ", IMEX T1/S2, 4 Picard, GMRES tol 1e-10", "fp64": out["fp64"],
                       "mixed": out["mixed"], "mixed_speedup": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
-                      "state_rel_drift": drift})
-    return {"steps_timed": steps, "mixed_speedup": cases[0]["mixed_speedup"], "cases": cases}
+                      "state_rel_drift": drift, "density_l1_rel_drift": l1drift, "all_steps_converged": ok})
+    return {"steps_timed": steps, "mixed_speedup": cases[0]["mixed_speedup"],
+            "bytes_model": "GMRES: the solve's count of vector sweeps (8 B per FP64 entry, 4 per FP32 basis entry); "
+                           "outside GMRES: 88 B/cell star + 136 B/cell per Picard pass + 48 B/cell closeout",
+            "cases": cases}
 
 
-def batch_leg(dev, steps=200):
+def hllcp_leg(dev, stream, steps=20):
+    """The explicit step with the low-Mach-corrected HLLC-P flux
+    (xie_am_hllc_p, 5-face pressure sensor): the Gresho vortex at 256^2,
+    M = 0.01 (CFL 0.5), and the shock-density bubble at 2560x640 (CFL 0.45);
+    CUDA events around each step, L2 flushed before each."""
+    import torch
+
+    from amrex_euler_allmach_explicit_imex_b200 import _lib, api
+    from amrex_euler_allmach_explicit_imex_b200.config import read_config
+
+    lib = _lib.load()
+    peak, _ = peaks()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    sink = torch.empty((), dtype=torch.float32, device=dev)
+    cases = [("gresho_vortex 256x256 periodic, M=0.01, xie_am_hllc_p, CFL 0.5",
+              dict(imex_kv(256, 0.01), **{"euler.method": "explicit", "euler.riemann": "xie_am_hllc_p",
+                                          "euler.cfl": 0.5})),
+             ("shock_density_bubble_2d 2560x640, xie_am_hllc_p, CFL 0.45",
+              dict(WORKLOAD_KV, **{"euler.riemann": "xie_am_hllc_p"}))]
+    res = []
+    for name, kv in cases:
+        cfg = read_config(kv).cfg
+        cells = cfg.n_cell[0] * cfg.n_cell[1]
+        with api.Context(cfg, arith="fast", device=dev.index or 0, stream=stream.cuda_stream) as ctx:
+            api.initialize_state(ctx)
+            t = 0.0
+            for _ in range(3):
+                dt = api.compute_euler_dt(ctx, t)
+                api.euler_fv_one_step(ctx, dt, t)
+                t += dt
+            ms = []
+            for k in range(steps):
+                dt = api.compute_euler_dt(ctx, t)
+                with torch.cuda.stream(stream):
+                    flush.fill_(float(k))
+                    sink.copy_(flush.sum())
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                _lib.check(lib.ecg_euler_fv_one_step(ctx.handle, dt, t, None), "euler_fv_one_step")
+                b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+                t += dt
+            d = api.compute_diagnostics(ctx)
+        us = 1e3 * sum(ms) / len(ms)
+        gbs = BYTES_PER_CELL * cells / (us * 1e-6) / 1e9
+        res.append({"workload": name, "cells": cells, "us_per_step": us, "value": cells / (us * 1e-6), "unit": UNIT,
+                    "achieved_gbs": gbs, "hbm_frac": gbs / peak,
+                    "state_ok": bool(d.nonfinite_count == 0 and d.rho_min > 0 and d.pressure_min > 0)})
+    return {"steps_timed": steps, "cases": res}
+
+
+def batch_leg(dev, stream, steps=200):
     """64 independent explicit O2 HLLC Riemann solves on the seeded grid ladder
     {64x64, 128x32, 256x256, 512x128, 1024x256}, one persistent launch per
-    step for the whole batch, CUDA graphs; cell-updates/s over `steps` steps."""
+    step for the whole batch, CUDA graphs; cell-updates/s over `steps` steps,
+    timed with CUDA events on the batch's stream."""
     import torch
 
     from amrex_euler_allmach_explicit_imex_b200 import api, workloads
 
     cfgs, states = workloads.riemann_batch(64, seed=0)
     cells = sum(c.cfg.n_cell[0] * c.cfg.n_cell[1] for c in cfgs)
-    with api.Batch(cfgs, device=dev.index or 0) as b:
+    with api.Batch(cfgs, device=dev.index or 0, stream=stream.cuda_stream) as b:
         for k, u in enumerate(states):
             b.upload(k, u)
         b.run(24)  # autotune and graph capture
         for k, u in enumerate(states):
             b.upload(k, u)
         torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         res = b.run(steps)
-        el = time.perf_counter() - t0
+        e1.record(stream)
+        e1.synchronize()
+        el = e0.elapsed_time(e1) * 1e-3
     ok = all(r.steps == steps and r.failed == 0 for r in res)
+    peak, _ = peaks()
     return {"workload": "64 Riemann solves, grids drawn (seed 0) from 64x64..1024x256, O2 HLLC FP64, CFL 0.5",
             "cells": cells, "steps": steps, "seconds": el, "value": cells * steps / el, "unit": UNIT,
-            "all_solves_completed": ok}
+            "hbm_frac": BYTES_PER_CELL * cells * steps / el / 1e9 / peak, "all_solves_completed": ok}
 
 
 def run_ours(args):
@@ -482,6 +569,32 @@ def run_ours(args):
     e2e_ms = max_over_ranks(dist, e_start.elapsed_time(e_end), dev)
     e2e_value = sum_over_ranks(dist, cells * e2e_k, dev) / (e2e_ms * 1e-3)
 
+    # The same calls on pageable host memory (an FArrayBox as AMReX allocates
+    # it, never registered with CUDA): the copies then go through the
+    # driver's staging buffers.
+    page_a = np.ascontiguousarray(host_a.numpy()).copy()
+    page_b = np.empty_like(page_a)
+    for _ in range(2):
+        dt = api.compute_euler_dt(ctx, te)
+        _lib.check(lib.ecg_euler_fv_one_step_host(ctx.handle, page_a.ctypes.data, page_b.ctypes.data, 0, 0, NX,
+                                                  NX * NY, dt, te, C.byref(deg)), "euler_fv_one_step_host")
+        page_a, page_b = page_b, page_a
+        te += dt
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    e_start.record(stream)
+    for _ in range(e2e_k):
+        dt = api.compute_euler_dt(ctx, te)
+        _lib.check(lib.ecg_euler_fv_one_step_host(ctx.handle, page_a.ctypes.data, page_b.ctypes.data, 0, 0, NX,
+                                                  NX * NY, dt, te, C.byref(deg)), "euler_fv_one_step_host")
+        page_a, page_b = page_b, page_a
+        te += dt
+    e_end.record(stream)
+    torch.cuda.synchronize(dev)
+    pg_ms = max_over_ranks(dist, e_start.elapsed_time(e_end), dev)
+    pg_value = sum_over_ranks(dist, cells * e2e_k, dev) / (pg_ms * 1e-3)
+
     line = None
     if rank == 0:
         cpu = None
@@ -506,7 +619,9 @@ def run_ours(args):
                          "traffic": traffic, "peak_source": peak_kind, "fp64": fp64,
                          "note": "algorithmic bytes = 64 B x 1,638,400 cells per launch; event time of the fused step kernel"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * cells,
-                    "d2h_bytes_per_step": 32 * cells},
+                    "d2h_bytes_per_step": 32 * cells, "host_memory": "pinned"},
+            "e2e_pageable": {"value": pg_value, "unit": UNIT, "h2d_bytes_per_step": 32 * cells,
+                             "d2h_bytes_per_step": 32 * cells, "host_memory": "pageable (numpy)"},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
@@ -514,7 +629,8 @@ def run_ours(args):
         }
         if world == 1 and not args.no_extra_legs:
             line["imex"] = imex_leg(dev, stream)
-            line["batched"] = batch_leg(dev)
+            line["hllcp"] = hllcp_leg(dev, stream)
+            line["batched"] = batch_leg(dev, stream)
         print(json.dumps(line))
     ctx.close()
     if dist is not None:
@@ -532,7 +648,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true", help="skip the IMEX and batched measurements")
-    ap.add_argument("--only", choices=["imex", "batched"], default=None,
+    ap.add_argument("--only", choices=["imex", "batched", "hllcp"], default=None,
                     help="run one of the extra legs alone (profiling) and print its JSON")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -545,7 +661,9 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         stream = torch.cuda.Stream(device=dev)
-        leg = imex_leg(dev, stream, steps=2) if args.only == "imex" else batch_leg(dev)
+        legs = {"imex": lambda: imex_leg(dev, stream, steps=2), "batched": lambda: batch_leg(dev, stream),
+                "hllcp": lambda: hllcp_leg(dev, stream)}
+        leg = legs[args.only]()
         print(json.dumps({"leg": args.only, **leg}))
         return 0
     return run_ours(args)

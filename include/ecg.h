@@ -52,7 +52,9 @@ typedef enum ecg_problem {
    * rho = 0.138, p = 1) on [0,4] x [0,1], post-shock inflow on the left,
    * outflow on the right, reflecting walls at y = 0 and y = 1, gamma = 1.4.
    * The reference's config reader rejects this geometry for
-   * shock_density_bubble_2d (config_reader.hpp:288-298). Explicit method only. */
+   * shock_density_bubble_2d (config_reader.hpp:288-298).  Both the explicit
+   * and the IMEX method run it; the IMEX step uses the bubble's source-map
+   * boundary policy with a reflecting wall at both y ends. */
   ECG_PROBLEM_SHOCK_BUBBLE_MACH122 = 7
 } ecg_problem;
 
@@ -149,12 +151,17 @@ typedef struct ecg_gpu_options {
   int32_t mixed_max_refinements; /* mixed: cycles, each opened with the true FP64 residual */
   int32_t tile_x;           /* column-strip kernel: rows each warp marches (0: sized so the grid fills one wave) */
   int32_t tile_y;           /* explicit kernel: 0 default (column strips, x- and y-faces
-                               evaluated together), 2 column strips with faces one at a
-                               time, 1 square 16x16 tiles, 8 or 16 the 32 x tile_y tiles */
+                               evaluated together, rows staged through shared memory),
+                               3 the same with rows loaded into registers, 2 column strips
+                               with faces one at a time, 1 square 16x16 tiles, 8 or 16 the
+                               32 x tile_y tiles */
   int32_t mixed_reorth;     /* mixed: Gram-Schmidt second pass (DGKS) of the FP32-basis cycles:
                                1 when ||w'|| < ||w||/sqrt(2), as the FP64 solve; 0 (default) only
                                when ||w'|| < 1e-3 ||w||, where the Pythagorean norm would lose digits */
   void* stream;             /* cudaStream_t to run on, NULL = context-owned stream */
+  int32_t deterministic;    /* 1: the GMRES grid sums run in a fixed block order, so repeated IMEX steps on
+                               the same inputs give the same bits (a little slower); 0 (default): atomic
+                               accumulation, whose order can change the last bits from run to run */
 } ecg_gpu_options;
 
 /* Diagnostics (core/basic_diagnostics.hpp:3-7). */
@@ -256,6 +263,9 @@ typedef struct ecg_imex_diag {
   double eq78_divergence_scaled_linf;
   double energy_closeout_delta_l1;
   double energy_closeout_delta_linf;
+  double gmres_vector_bytes;          /* bytes the step's GMRES sweeps read and write, counted from the iterations
+                                         run: every sweep over a vector of n rows counts n entries of its width
+                                         (not in the reference) */
 } ecg_imex_diag;
 
 /* Result of a device-resident time loop (driver_main.hpp:224-333). */
@@ -519,8 +529,9 @@ ecg_status ecg_explicit_step_device(ecg_ctx* ctx, const double* u0, double dt, d
  * context and no device or host allocation, for callers that cannot allocate
  * inside their time loop (an AMReX GPU build whose arena reserves most of HBM
  * at start-up and whose stream pipeline a cudaFree would synchronise).
- * state_in/state_out: distinct device arrays in the Array4 layout of
- * ecg_upload_state (same lo, jstride, nstride for both); ghost cells come from
+ * state_in/state_out: device arrays in the Array4 layout of ecg_upload_state
+ * (same lo, jstride, nstride for both) that share no byte (4 planes of nstride
+ * doubles from each base; overlap is ECG_ERR_BAD_ARG); ghost cells come from
  * the boundary conditions of cfg.  opt may be NULL (defaults; opt->stream is
  * the stream the work is queued on, opt->device the device).  Scratch lives
  * in one static device array of ECG_NOALLOC_SCRATCH_BYTES per device: the
@@ -528,7 +539,8 @@ ecg_status ecg_explicit_step_device(ecg_ctx* ctx, const double* u0, double dt, d
  * ring and are rejected with ECG_ERR_BAD_ARG beyond that; the others have no
  * size limit.  Calls that overlap in time on one device race on that scratch.
  * The first call on a device looks the scratch up (make it before any stream
- * capture).  hllc_degenerate_count (may be NULL) synchronises the stream.  On
+ * capture) and keeps its address until exit: after a cudaDeviceReset of that
+ * device the entry point must not be called on it again.  hllc_degenerate_count (may be NULL) synchronises the stream.  On
  * failure a message is written to err (err_len bytes, may be NULL). */
 #define ECG_NOALLOC_SCRATCH_BYTES (8u << 20)
 ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gpu_options* opt,

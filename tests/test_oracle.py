@@ -197,3 +197,46 @@ def test_output_fixture_is_the_reference_writers(ref, tmp_path):
         ref.write_final_csv(d[name + "_u"], int(step), float(time), p, tuple(trial))
         with open(p) as f:
             assert f.read() == str(d[name + "_csv"])
+
+
+def _baseline(name):
+    z = golden_io.load("baseline_cases.npz")
+    return {k[len(name) + 1:]: z[k] for k in z.files if k.startswith(name + "_")}
+
+
+def test_baseline_explicit_hllcp_fixture_is_the_oracle_step(oracle):
+    """The restatement reproduces the reference's explicit HLLC-P step of the
+    256^2 Gresho vortex (M = 0.01) bit for bit, from its own initial state."""
+    c = _baseline("gresho256_m0p01_hllcp")
+    cfg = read_config(golden_io.kv_of(c["kv"])).cfg
+    u0 = oracle.initialize(cfg)
+    assert oracle.euler_dt(cfg, u0, 0.0) == float(c["dt"])
+    u1, deg = oracle.step(cfg, u0, float(c["dt"]), 0.0)
+    assert np.array_equal(u1, c["u1"])
+    assert deg == int(c["deg"])
+
+
+def test_baseline_bubble_imex_fixture_vs_oracle(oracle):
+    """The restated IMEX step on the 640 x 160 bubble against the reference's
+    (GMRES rounding: 1e-9 relative), with the reference's dt."""
+    c = _baseline("bubble640x160")
+    cfg = read_config(golden_io.kv_of(c["kv"])).cfg
+    u0 = oracle.initialize(cfg)
+    dt, _ = oracle.imex_dt(cfg, u0)
+    assert dt == float(c["dt"])
+    u1, d = oracle.imex_step(cfg, u0, dt)
+    assert d.solver_status in (1, 2)
+    assert golden_io.state_rel_err(u1, c["u1"]) <= 1e-9
+
+
+def test_gresho_l1_restatement_matches_reference(oracle, ref):
+    """compute_gresho_metrics' density L1 error (diagnostic_metrics_timestep.hpp:
+    150-225), restated in the oracle, on a perturbed periodic Gresho state."""
+    kv = golden_io.load("baseline_cases.npz")["gresho256_m0p1_kv"]
+    text = golden_io.kv_of(kv).replace("amr.n_cell=256 256", "amr.n_cell=48 40")
+    cfg = ref.configure(text)
+    rng = np.random.default_rng(3)
+    u = ref.initialize() * (1 + 1e-3 * rng.standard_normal((4, 40, 48)))
+    want = ref.gresho_density_l1(u)
+    assert want > 0
+    assert oracle.gresho_density_l1(cfg, u) == pytest.approx(want, rel=1e-13)
