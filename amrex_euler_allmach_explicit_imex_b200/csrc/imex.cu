@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <limits>
 
 #include "ctx.h"
@@ -312,11 +313,12 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
       d.solver_status = g.breakdown ? ECG_SOLVER_GMRES_BREAKDOWN_NOT_CONVERGED : ECG_SOLVER_LINEAR_SOLVE_NOT_CONVERGED;
       return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
     }
-    // p <- x, eq54 momentum refresh (imex_source_map_step.hpp:536-564)
+    // p <- x, eq54 momentum refresh (imex_source_map_step.hpp:536-564), in one
+    // sweep: K from x, then x becomes the pressure buffer (no copy)
     if (!reset_stats(c)) return ECG_ERR_CUDA;
-    if (!ecgi::cuda_ok(c, ops->p_update(n, im->p, im->x, im->d_st, s), "p update")) return ECG_ERR_CUDA;
-    if (!ecgi::cuda_ok(c, ops->momentum(m, im->S, im->p, dt, idx, idy, im->K, im->d_st, s), "momentum"))
+    if (!ecgi::cuda_ok(c, ops->refresh(m, im->p, im->x, im->S, dt, idx, idy, im->K, im->d_st, s), "refresh"))
       return ECG_ERR_CUDA;
+    std::swap(im->p, im->x);
     if (!fetch_stats(c)) return ECG_ERR_CUDA;
     d.kinetic_lag_nonfinite_count = static_cast<int>(st.k_nonfinite);
     if (st.k_nonfinite > 0) {

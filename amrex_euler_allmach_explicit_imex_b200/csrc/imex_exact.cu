@@ -6,4 +6,4 @@
 const EcgImexOps ecg_imex_exact_ops = {ecg_exact::imex_star,     ecg_exact::imex_faces,    ecg_exact::imex_rhs,
                                        ecg_exact::imex_matrix,
                                        ecg_exact::imex_p_update, ecg_exact::imex_momentum, ecg_exact::imex_closeout,
-                                       ecg_exact::imex_eq78};
+                                       ecg_exact::imex_eq78, ecg_exact::imex_refresh};

@@ -65,6 +65,9 @@ struct EcgImexOps {
                           double dt, double* out, EcgImexStats* st, cudaStream_t s);
   cudaError_t (*eq78)(const EcgImexMap& m, const EcgGrid& G, const double* S, const double* K, EcgImexStats* st,
                       cudaStream_t s);
+  // p_update and momentum in one sweep, K from x; the caller swaps p and x
+  cudaError_t (*refresh)(const EcgImexMap& m, const double* p_old, const double* x, const double* S, double dt,
+                         double idx, double idy, double* K, EcgImexStats* st, cudaStream_t s);
 };
 
 extern const EcgImexOps ecg_imex_exact_ops;

@@ -720,6 +720,43 @@ __global__ void __launch_bounds__(NT) imex_momentum_kernel(const EcgImexMap m, c
   ECG_RED_ADD_I(st->k_nonfinite, nf);
 }
 
+// The end of a Picard pass in one sweep: the delta statistics of the new
+// pressure x against the previous p (imex_p_update_kernel) and the eq54
+// momentum from x (imex_momentum_kernel), bit for bit the two kernels in
+// sequence.  x is not copied into p: the caller swaps the two buffers, so x
+// becomes the pass's pressure.
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_refresh_kernel(const EcgImexMap m, const double* __restrict__ p_old,
+                                                          const double* __restrict__ x, const double* __restrict__ S,
+                                                          const double dt, const double idx, const double idy,
+                                                          double* __restrict__ K, EcgImexStats* __restrict__ st)
+{
+  __shared__ Shared sh;
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  unsigned long long dl = okey(0.0), pm = okey(1.0);
+  double d2 = 0.0;
+  long long nf = 0;
+  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
+       r += static_cast<long long>(gridDim.x) * NT) {
+    const double o = p_old[r], nv = x[r];
+    const double d = nv - o;
+    dl = umax64(dl, okey(fabs(d)));
+    d2 += d * d;
+    pm = umax64(pm, umax64(okey(fabs(o)), okey(fabs(nv))));
+    const int j = static_cast<int>(static_cast<unsigned>(r) / static_cast<unsigned>(m.nx)), i = static_cast<int>(r) - j * m.nx;
+    const double gx = 0.5 * (p_b(m, x, i + 1, j) - p_b(m, x, i - 1, j)) * idx;
+    const double gy = 0.5 * (p_b(m, x, i, j + 1) - p_b(m, x, i, j - 1)) * idy;
+    const double k0 = S[r + n] - dt * gx, k1 = S[r + 2 * n] - dt * gy;
+    K[r] = k0;
+    K[r + n] = k1;
+    if (!isfinite(k0) || !isfinite(k1)) ++nf;
+  }
+  ECG_RED_MAX(st->delta_linf_key, dl);
+  ECG_RED_ADD_D(st->delta_l2_sum, d2);
+  ECG_RED_MAX(st->pmax_key, pm);
+  ECG_RED_ADD_I(st->k_nonfinite, nf);
+}
+
 // ---- closeout ------------------------------------------------------------------------
 
 // evaluate_source_map_final (imex_source_map_step.hpp:75-188): the
@@ -983,6 +1020,14 @@ inline cudaError_t imex_momentum(const EcgImexMap& m, const double* S, const dou
 {
   const long long n = static_cast<long long>(m.nx) * m.ny;
   imexk::imex_momentum_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, p, dt, idx, idy, K, st);
+  return cudaGetLastError();
+}
+
+inline cudaError_t imex_refresh(const EcgImexMap& m, const double* p_old, const double* x, const double* S, double dt,
+                                double idx, double idy, double* K, EcgImexStats* st, cudaStream_t s)
+{
+  const long long n = static_cast<long long>(m.nx) * m.ny;
+  imexk::imex_refresh_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, p_old, x, S, dt, idx, idy, K, st);
   return cudaGetLastError();
 }
 

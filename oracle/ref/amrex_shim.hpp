@@ -22,7 +22,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cctype>
 #include <cstdlib>
+#include <cstring>
 #include <limits>
 #include <map>
 #include <stdexcept>
@@ -77,22 +79,33 @@ inline std::string*& print_sink()
   static std::string* sink = nullptr;
   return sink;
 }
+// A driver executable (Initialize) prints to stdout instead.
+inline bool& print_to_stdout()
+{
+  static bool on = false;
+  return on;
+}
+inline void print_text(const char* s, std::size_t n)
+{
+  if (print_to_stdout()) std::fwrite(s, 1, n, stdout);
+  else if (print_sink()) print_sink()->append(s, n);
+}
 struct Print {
   template <class T>
   Print& operator<<(const T&) { return *this; }
   Print& operator<<(const char* s)
   {
-    if (print_sink()) print_sink()->append(s);
+    print_text(s, std::strlen(s));
     return *this;
   }
   Print& operator<<(const std::string& s)
   {
-    if (print_sink()) print_sink()->append(s);
+    print_text(s.data(), s.size());
     return *this;
   }
   Print& operator<<(char c)
   {
-    if (print_sink()) print_sink()->push_back(c);
+    print_text(&c, 1);
     return *this;
   }
   Print& operator<<(double v) { return num("%.17g", v); }
@@ -106,20 +119,16 @@ struct Print {
  private:
   Print& num(const char* fmt, double v)
   {
-    if (print_sink()) {
-      char b[64];
-      std::snprintf(b, sizeof(b), fmt, v);
-      print_sink()->append(b);
-    }
+    char b[64];
+    const int n = std::snprintf(b, sizeof(b), fmt, v);
+    print_text(b, static_cast<std::size_t>(n));
     return *this;
   }
   Print& inum(long long v)
   {
-    if (print_sink()) {
-      char b[32];
-      std::snprintf(b, sizeof(b), "%lld", v);
-      print_sink()->append(b);
-    }
+    char b[32];
+    const int n = std::snprintf(b, sizeof(b), "%lld", v);
+    print_text(b, static_cast<std::size_t>(n));
     return *this;
   }
 };
@@ -463,5 +472,31 @@ class ParmParse {
     return true;
   }
 };
+
+// The executable's start-up as AMReX does it for the driver: every
+// "key=value ..." argument becomes a ParmParse entry (values split at
+// whitespace), and Print goes to stdout.
+inline void Initialize(int& argc, char**& argv)
+{
+  auto& table = parmparse_table();
+  table.clear();
+  for (int a = 1; a < argc; ++a) {
+    const std::string arg(argv[a]);
+    const auto eq = arg.find('=');
+    if (eq == std::string::npos || eq == 0) continue;
+    std::vector<std::string> vals;
+    std::size_t k = eq + 1;
+    while (k < arg.size()) {
+      while (k < arg.size() && std::isspace(static_cast<unsigned char>(arg[k]))) ++k;
+      std::size_t e = k;
+      while (e < arg.size() && !std::isspace(static_cast<unsigned char>(arg[e]))) ++e;
+      if (e > k) vals.push_back(arg.substr(k, e - k));
+      k = e;
+    }
+    table[arg.substr(0, eq)] = vals;
+  }
+  print_to_stdout() = true;
+}
+inline void Finalize() { std::fflush(stdout); }
 
 }  // namespace amrex
