@@ -163,8 +163,13 @@ IMEX_DIAG_REAL_FIELDS = [
 ]
 
 
+# fields after the reals, not in the reference
+IMEX_DIAG_TAIL_FIELDS = ["gmres_fp64_fallbacks", "pad_end"]
+
+
 class ImexDiag(C.Structure):
-    _fields_ = [(n, C.c_int32) for n in IMEX_DIAG_INT_FIELDS] + [(n, C.c_double) for n in IMEX_DIAG_REAL_FIELDS]
+    _fields_ = ([(n, C.c_int32) for n in IMEX_DIAG_INT_FIELDS] + [(n, C.c_double) for n in IMEX_DIAG_REAL_FIELDS] +
+                [(n, C.c_int32) for n in IMEX_DIAG_TAIL_FIELDS])
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

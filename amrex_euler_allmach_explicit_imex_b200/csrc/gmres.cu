@@ -832,8 +832,8 @@ __device__ __forceinline__ double sweep_next(Rows rw, const Basis<TV>& bs, const
 template <typename TV, bool RES>
 __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec, const double* x0vec, double* xvec,
                              TV* __restrict__ V, double* __restrict__ w,
-                             double* __restrict__ rres, int kmax, double tol, double restart_rtol, unsigned int& gen,
-                             unsigned int& nred, unsigned int& nset, double* shbase)
+                             double* __restrict__ rres, int kmax, double tol, double restart_rtol, int reorth,
+                             unsigned int& gen, unsigned int& nred, unsigned int& nset, double* shbase)
 {
   const long long n = a.n;
   const Rows rw = own_rows(n);
@@ -983,7 +983,7 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     // may take it only under severe cancellation: their basis rounding
     // (2^-24) already bounds orthogonality far above what the second pass
     // restores, and a cycle only has to reduce its residual by inner_rtol.
-    const double eta = (sizeof(TV) == 8 || a.reorth) ? 0.5 : 1.0e-6;
+    const double eta = (sizeof(TV) == 8 || reorth) ? 0.5 : 1.0e-6;
     if (!(nn2 >= eta * sw)) {
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
       if (wide) sweep_combine<TV, true, 2>(rw, bs, S.coef, j + 1, w, w);
@@ -1133,7 +1133,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   }
   if constexpr (!MIXED) {
     const SolveState st =
-        krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, gen, nred, nset, sh);
+        krylov<double, RES>(a, a.b, a.x0, a.x, a.V, a.w, a.r, limit > 0 ? limit : 0, a.tol, 0.0, 1, gen, nred, nset, sh);
     out.iterations = st.best_it;
     out.converged = st.converged;
     out.breakdown = st.breakdown;
@@ -1146,7 +1146,13 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   } else {
     // Cycles of the FP32-basis solve; each opens with the true FP64 residual
     // of the current iterate (x0, then x) and the reference's stopping rule.
+    // A cycle that cut the true residual by less than kStall (its recurrence
+    // believed an FP32 basis that had lost its orthogonality) turns the DGKS
+    // second pass on for the cycles that follow.
+    constexpr double kStall = 0.1;
     int total = 0, cycles = 0;
+    int reorth = a.reorth;
+    double prev_r0 = __builtin_huge_val();
     const double* xin = a.x0;
     SolveState st;
     std::memset(&st, 0, sizeof(st));
@@ -1155,12 +1161,17 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
       const int left = limit - total;
       const bool last = cycles + 1 >= a.max_refine;
       const int kin = per_cycle < left ? per_cycle : left;
-      st = krylov<float, RES>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol, gen,
-                              nred, nset, sh);
+      st = krylov<float, RES>(a, a.b, xin, a.x, a.V32, a.w, a.r, kin > 0 ? kin : 0, a.tol, last ? 0.0 : a.inner_rtol,
+                              reorth, gen, nred, nset, sh);
       if (cycles == 0) {
         out.initial_linf = st.r0_linf;
         out.b_linf = st.b_linf;
       }
+      if (cycles > 0 && !(st.r0_linf <= kStall * prev_r0) && !reorth) {
+        reorth = 1;
+        out.stalled_cycles += 1;
+      }
+      prev_r0 = st.r0_linf;
       ++cycles;
       out.iterations = total + st.best_it;
       total += st.it;

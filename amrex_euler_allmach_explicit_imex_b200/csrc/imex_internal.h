@@ -96,7 +96,7 @@ struct EcgGmresResult {
   int timeout;         // a bounded grid barrier gave up
   int inner_iterations;
   int refinements;
-  int pad;
+  int stalled_cycles;  // mixed: cycles after which the DGKS second pass was turned on (0 or 1)
   double residual_linf;
   double relative_residual_linf;
   // true residuals, as pressure_residual computes them: ||A x0 - b||inf and

@@ -465,6 +465,69 @@ def batch_leg(dev, stream, steps=200):
             "hbm_frac": BYTES_PER_CELL * cells * steps / el / 1e9 / peak, "all_solves_completed": ok}
 
 
+def run_slab(args):
+    """--slab: ONE grid (--slab-grid, default 10240x2560 of the bubble
+    problem) split over the N ranks as x-slabs (slab.SlabSolver): every step
+    packs the edge columns, swaps them with the neighbours over NCCL, steps
+    each slab and takes the global dt as the minimum over ranks.  Strong
+    scaling: value = the whole grid's cell-updates / (max over ranks of the
+    event-timed region), which includes the halo exchange and the dt
+    all-reduce."""
+    import torch
+
+    from amrex_euler_allmach_explicit_imex_b200 import slab
+    from amrex_euler_allmach_explicit_imex_b200.config import read_config
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(world, "nccl")
+    dev = torch.device("cuda", local)
+    nx, ny = (int(v) for v in args.slab_grid.lower().split("x"))
+    kv = dict(WORKLOAD_KV, **{"amr.n_cell": f"{nx} {ny}"})
+    cfg = read_config(kv).cfg
+    solver = slab.SlabSolver(cfg, device=local, arith="fast")
+    solver.initialize_state()
+    t = 0.0
+    for _ in range(args.warmup):
+        dt = solver.compute_euler_dt(t)
+        solver.euler_fv_one_step(dt, t)
+        t += dt
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    stream = solver.stream
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dt = solver.compute_euler_dt(t)
+        solver.euler_fv_one_step(dt, t)
+        t += dt
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), dev)
+    cells = nx * ny
+    value = cells * args.steps / (ms * 1e-3)
+    d = solver.ctx.download()
+    ok = bool(np.isfinite(d).all())
+    solver.close()
+    if rank == 0:
+        peak, _ = peaks()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (the shock-density bubble's initializer)",
+                "config": {"workload": f"shock_density_bubble_2d {nx}x{ny}, explicit O2 HLLC, FP64, one grid in "
+                                       f"{world} x-slabs with a 2-column NCCL halo exchange per step",
+                           "grid": [nx, ny], "parallelism": f"slabs{world}"},
+                "hbm_frac_per_gpu": BYTES_PER_CELL * cells / world / (ms / args.steps * 1e-3) / 1e9 / peak,
+                "state_ok": ok}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
 
@@ -648,6 +711,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra-legs", action="store_true", help="skip the IMEX and batched measurements")
+    ap.add_argument("--slab", action="store_true",
+                    help="strong scaling: one grid split over the ranks as x-slabs with an NCCL halo exchange")
+    ap.add_argument("--slab-grid", default="10240x2560")
     ap.add_argument("--only", choices=["imex", "batched", "hllcp"], default=None,
                     help="run one of the extra legs alone (profiling) and print its JSON")
     args = ap.parse_args()
@@ -655,6 +721,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.slab:
+        return run_slab(args)
     if args.only:
         import torch
 

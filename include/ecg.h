@@ -266,6 +266,10 @@ typedef struct ecg_imex_diag {
   double gmres_vector_bytes;          /* bytes the step's GMRES sweeps read and write, counted from the iterations
                                          run: every sweep over a vector of n rows counts n entries of its width
                                          (not in the reference) */
+  int32_t gmres_fp64_fallbacks;       /* mixed precision: Picard solves the FP32-basis cycles left above the
+                                         tolerance and the FP64 solve finished from their iterate (not in the
+                                         reference) */
+  int32_t pad_end;
 } ecg_imex_diag;
 
 /* Result of a device-resident time loop (driver_main.hpp:224-333). */
