@@ -260,9 +260,8 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
   for (int pic = 0; pic < c->cfg.imex_picard_iterations; ++pic) {
     // pressure system (source_map_build_pressure_system, imex_source_map_step.hpp:8-38,464-497)
     if (!reset_stats(c)) return ECG_ERR_CUDA;
-    if (!ecgi::cuda_ok(c, ops->faces(m, im->S, im->p, im->K, im->hx, im->hy, nullptr, nullptr, 0, s), "faces"))
-      return ECG_ERR_CUDA;
-    if (!ecgi::cuda_ok(c, ops->rhs(m, im->S, im->K, im->hx, im->hy, dt, idx, idy, im->rhs, im->d_st, s), "rhs"))
+    if (!ecgi::cuda_ok(c, ops->assemble(m, im->S, im->p, im->K, im->hx, im->hy, dt, idx, idy, im->rhs, im->d_st, s),
+                       "assemble"))
       return ECG_ERR_CUDA;
     if (!fetch_stats(c)) return ECG_ERR_CUDA;
     d.pressure_matrix_rows = static_cast<int>(n);

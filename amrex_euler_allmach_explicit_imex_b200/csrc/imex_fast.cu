@@ -3,7 +3,6 @@
 #define ECG_NS ecg_fast
 #include "imex_kernels.cuh"
 
-const EcgImexOps ecg_imex_fast_ops = {ecg_fast::imex_star,     ecg_fast::imex_faces,    ecg_fast::imex_rhs,
-                                      ecg_fast::imex_matrix,
-                                      ecg_fast::imex_p_update, ecg_fast::imex_momentum, ecg_fast::imex_closeout,
-                                      ecg_fast::imex_eq78, ecg_fast::imex_refresh};
+const EcgImexOps ecg_imex_fast_ops = {ecg_fast::imex_star,     ecg_fast::imex_faces, ecg_fast::imex_matrix,
+                                      ecg_fast::imex_closeout, ecg_fast::imex_eq78,  ecg_fast::imex_assemble,
+                                      ecg_fast::imex_refresh};

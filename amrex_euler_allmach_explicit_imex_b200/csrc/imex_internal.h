@@ -53,18 +53,17 @@ struct EcgImexOps {
                       EcgImexStats* st, cudaStream_t s);
   cudaError_t (*faces)(const EcgImexMap& m, const double* S, const double* p, const double* K, double* fx, double* fy,
                        unsigned char* fxf, unsigned char* fyf, int mode, cudaStream_t s);
-  cudaError_t (*rhs)(const EcgImexMap& m, const double* S, const double* K, const double* hx, const double* hy,
-                     double dt, double idx, double idy, double* rhs, EcgImexStats* st, cudaStream_t s);
   cudaError_t (*matrix)(const EcgImexMap& m, const double* hx, const double* hy, double dt, double idx, double idy,
                         EcgImexStats* st, cudaStream_t s);
-  cudaError_t (*p_update)(long long n, double* p, const double* x, EcgImexStats* st, cudaStream_t s);
-  cudaError_t (*momentum)(const EcgImexMap& m, const double* S, const double* p, double dt, double idx, double idy,
-                          double* K, EcgImexStats* st, cudaStream_t s);
   cudaError_t (*closeout)(const EcgImexMap& m, const EcgGrid& G, const double* S, const double* p, const double* K,
                           const double* fx, const double* fy, const unsigned char* fxf, const unsigned char* fyf,
                           double dt, double* out, EcgImexStats* st, cudaStream_t s);
   cudaError_t (*eq78)(const EcgImexMap& m, const EcgGrid& G, const double* S, const double* K, EcgImexStats* st,
                       cudaStream_t s);
+  // faces (mode 0) and rhs in one launch
+  cudaError_t (*assemble)(const EcgImexMap& m, const double* S, const double* p, const double* K, double* hx,
+                          double* hy, double dt, double idx, double idy, double* rhs, EcgImexStats* st,
+                          cudaStream_t s);
   // p_update and momentum in one sweep, K from x; the caller swaps p and x
   cudaError_t (*refresh)(const EcgImexMap& m, const double* p_old, const double* x, const double* S, double dt,
                          double idx, double idy, double* K, EcgImexStats* st, cudaStream_t s);

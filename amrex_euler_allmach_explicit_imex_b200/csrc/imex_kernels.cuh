@@ -416,79 +416,123 @@ __device__ __forceinline__ void row_terms(const EcgImexMap& m, const double* __r
   }
 }
 
-// Right-hand side of source_map_pressure_row_data
-// (imex_source_map_helpers.hpp:488-570) with its nonfinite count.
-template <int NT>
-__global__ void __launch_bounds__(NT) imex_rhs_kernel(const EcgImexMap m, const double* __restrict__ S,
-                                                      const double* __restrict__ K, const double* __restrict__ hx,
-                                                      const double* __restrict__ hy, const double dt, const double idx,
-                                                      const double idy, double* __restrict__ rhs,
-                                                      EcgImexStats* __restrict__ st)
+// Right-hand side of row (i, j) of source_map_pressure_row_data
+// (imex_source_map_helpers.hpp:488-570) from the row's four face enthalpies;
+// rnf counts its nonfinite terms.
+__device__ __forceinline__ double rhs_row(const EcgImexMap& m, const double* __restrict__ S,
+                                          const double* __restrict__ K, double he, double hw, double hn, double hs,
+                                          int i, int j, double dt, double idx, double idy, double xc, double yc,
+                                          int& rnf)
 {
-  __shared__ Shared sh;
-  const int n = m.nx * m.ny;  // rows fit 32-bit indices (the GMRES workspace rejects larger systems)
   const double gm1 = m.gamma - 1.0;
-  const double xc = 0.25 * dt * dt * idx * idx, yc = 0.25 * dt * dt * idy * idy;
-  long long nonfinite = 0;
-  unsigned long long bmax = okey(0.0);
-  for (int r = blockIdx.x * NT + threadIdx.x; r < n; r += gridDim.x * NT) {
-    const int j = r / m.nx, i = r - j * m.nx;
-    const double he = hx[static_cast<long long>(j) * (m.nx + 1) + i + 1];
-    const double hw = hx[static_cast<long long>(j) * (m.nx + 1) + i];
-    const double hn = hy[static_cast<long long>(j + 1) * m.nx + i];
-    const double hs = hy[static_cast<long long>(j) * m.nx + i];
-    int rnf = 0;
-    double b = 0.0;
-    if (!isfinite(he) || !isfinite(hw) || !isfinite(hn) || !isfinite(hs)) ++rnf;
-    {
-      const int ci[11] = {i, i + 2, i + 1, i, i - 1, i - 2, i, i, i, i, i};
-      const double cv[11] = {1.0 / gm1, -xc * he, -xc * (he - hw), xc * (he + hw), xc * (he - hw),
-                             -xc * hw, -yc * hn, -yc * (hn - hs), yc * (hn + hs), yc * (hn - hs), -yc * hs};
+  rnf = 0;
+  double b = 0.0;
+  if (!isfinite(he) || !isfinite(hw) || !isfinite(hn) || !isfinite(hs)) ++rnf;
+  {
+    const int ci[11] = {i, i + 2, i + 1, i, i - 1, i - 2, i, i, i, i, i};
+    const double cv[11] = {1.0 / gm1, -xc * he, -xc * (he - hw), xc * (he + hw), xc * (he - hw),
+                           -xc * hw, -yc * hn, -yc * (hn - hs), yc * (hn + hs), yc * (hn - hs), -yc * hs};
 #pragma unroll
-      for (int q = 0; q < 11; ++q) {
-        if (m.bubble && !m.px && ci[q] < 0) {
-          const double c = -cv[q] * m.p_fixed;
-          b += c;
-          if (!isfinite(c)) ++rnf;
-        } else if (!isfinite(cv[q])) {
-          ++rnf;
-        }
+    for (int q = 0; q < 11; ++q) {
+      if (m.bubble && !m.px && ci[q] < 0) {
+        const double c = -cv[q] * m.p_fixed;
+        b += c;
+        if (!isfinite(c)) ++rnf;
+      } else if (!isfinite(cv[q])) {
+        ++rnf;
       }
     }
-    const Cons s = star_at(m, S, i, j);
-    double k0, k1;
-    m_at(m, K, i, j, k0, k1);
-    const double kin = 0.5 * (k0 * k0 + k1 * k1) / s.rho;
-    double v;
-    v = s.E;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    v = -kin;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    v = -0.5 * dt * idx * he * state_b(m, S, i + 1, j).mx;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    v = -0.5 * dt * idx * (he - hw) * s.mx;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    v = 0.5 * dt * idx * hw * state_b(m, S, i - 1, j).mx;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    v = -0.5 * dt * idy * hn * state_b(m, S, i, j + 1).my;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    v = -0.5 * dt * idy * (hn - hs) * s.my;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    v = 0.5 * dt * idy * hs * state_b(m, S, i, j - 1).my;
-    if (!isfinite(v)) ++rnf;
-    b += v;
-    if (!isfinite(b)) ++rnf;
-    rhs[r] = b;
-    nonfinite += rnf;
-    if (isfinite(b)) bmax = umax64(bmax, okey(fabs(b)));
-    else bmax = okey(kInf);
+  }
+  const Cons s = star_at(m, S, i, j);
+  double k0, k1;
+  m_at(m, K, i, j, k0, k1);
+  const double kin = 0.5 * (k0 * k0 + k1 * k1) / s.rho;
+  double v;
+  v = s.E;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  v = -kin;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  v = -0.5 * dt * idx * he * state_b(m, S, i + 1, j).mx;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  v = -0.5 * dt * idx * (he - hw) * s.mx;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  v = 0.5 * dt * idx * hw * state_b(m, S, i - 1, j).mx;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  v = -0.5 * dt * idy * hn * state_b(m, S, i, j + 1).my;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  v = -0.5 * dt * idy * (hn - hs) * s.my;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  v = 0.5 * dt * idy * hs * state_b(m, S, i, j - 1).my;
+  if (!isfinite(v)) ++rnf;
+  b += v;
+  if (!isfinite(b)) ++rnf;
+  return b;
+}
+
+// The assembly of one Picard pass in one kernel: the eq46 face enthalpies
+// (imex_face_kernel, mode 0) and the right-hand side of
+// source_map_pressure_row_data (imex_source_map_helpers.hpp:488-570) with its
+// nonfinite count.  A block takes a tile of AX columns x AY rows of cells:
+// every thread evaluates the x-face on its cell's left and the y-face below
+// it, the tile's right x-faces and top y-faces are evaluated once more by 40
+// threads (they belong to the neighbour tiles, which store them), and the
+// rows' right-hand sides read all four faces from shared memory instead of
+// from global memory.  Tiles run over the face columns 0 .. nx and rows
+// 0 .. ny.
+constexpr int AX = 32, AY = 8;
+template <int NT>
+__global__ void __launch_bounds__(NT) imex_assemble_kernel(const EcgImexMap m, const double* __restrict__ S,
+                                                           const double* __restrict__ p, const double* __restrict__ K,
+                                                           double* __restrict__ hx, double* __restrict__ hy,
+                                                           const double dt, const double idx, const double idy,
+                                                           double* __restrict__ rhs, EcgImexStats* __restrict__ st)
+{
+  static_assert(NT == AX * AY, "one thread per cell of the tile");
+  __shared__ Shared sh;
+  __shared__ double fx[AY][AX + 1];
+  __shared__ double fy[AY + 1][AX];
+  const int tx = threadIdx.x % AX, ty = threadIdx.x / AX;
+  const int c0 = blockIdx.x * AX, j0 = blockIdx.y * AY;
+  const int i = c0 + tx, j = j0 + ty;
+  const int nx = m.nx, ny = m.ny;
+  // the faces of the tile's own cells (and the domain's last face column/row)
+  if (j < ny && i <= nx) {
+    const double h = face_detail(m, S, p, K, i - 1, j, i, j, 0).h_hat;
+    hx[static_cast<long long>(j) * (nx + 1) + i] = h;
+    fx[ty][tx] = h;
+  }
+  if (i < nx && j <= ny) {
+    const double h = face_detail(m, S, p, K, i, j - 1, i, j, 1).h_hat;
+    hy[static_cast<long long>(j) * nx + i] = h;
+    fy[ty][tx] = h;
+  }
+  // the neighbour tiles' faces the tile's rows also need: column c0 + AX of
+  // x-faces (threads 0 .. AY-1), row j0 + AY of y-faces (threads 32 .. 63)
+  if (threadIdx.x < AY) {
+    const int jj = j0 + threadIdx.x, ii = c0 + AX;
+    if (jj < ny && ii <= nx) fx[threadIdx.x][AX] = face_detail(m, S, p, K, ii - 1, jj, ii, jj, 0).h_hat;
+  } else if (threadIdx.x >= 32 && threadIdx.x < 32 + AX) {
+    const int ii = c0 + threadIdx.x - 32, jj = j0 + AY;
+    if (ii < nx && jj <= ny) fy[AY][threadIdx.x - 32] = face_detail(m, S, p, K, ii, jj - 1, ii, jj, 1).h_hat;
+  }
+  __syncthreads();
+  long long nonfinite = 0;
+  unsigned long long bmax = okey(0.0);
+  if (i < nx && j < ny) {
+    const double xc = 0.25 * dt * dt * idx * idx, yc = 0.25 * dt * dt * idy * idy;
+    int rnf;
+    const double b = rhs_row(m, S, K, fx[ty][tx + 1], fx[ty][tx], fy[ty + 1][tx], fy[ty][tx], i, j, dt, idx, idy, xc,
+                             yc, rnf);
+    rhs[static_cast<long long>(j) * nx + i] = b;
+    nonfinite = rnf;
+    bmax = isfinite(b) ? okey(fabs(b)) : okey(kInf);
   }
   ECG_RED_ADD_I(st->row_nonfinite, nonfinite);
   ECG_RED_MAX(st->rhs_linf_key, bmax);
@@ -673,58 +717,12 @@ __global__ void __launch_bounds__(NT) imex_matrix_edge_kernel(const EcgImexMap m
 
 // ---- p update and eq54 momentum -----------------------------------------------------------
 
-// p <- x with the Picard delta statistics (imex_source_map_step.hpp:536-547).
-template <int NT>
-__global__ void __launch_bounds__(NT) imex_p_update_kernel(long long n, double* __restrict__ p,
-                                                           const double* __restrict__ x, EcgImexStats* __restrict__ st)
-{
-  __shared__ Shared sh;
-  unsigned long long dl = okey(0.0), pm = okey(1.0);
-  double d2 = 0.0;
-  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
-       r += static_cast<long long>(gridDim.x) * NT) {
-    const double o = p[r], nv = x[r];
-    const double d = nv - o;
-    dl = umax64(dl, okey(fabs(d)));
-    d2 += d * d;
-    pm = umax64(pm, umax64(okey(fabs(o)), okey(fabs(nv))));
-    p[r] = nv;
-  }
-  ECG_RED_MAX(st->delta_linf_key, dl);
-  ECG_RED_ADD_D(st->delta_l2_sum, d2);
-  ECG_RED_MAX(st->pmax_key, pm);
-}
-
+// The end of a Picard pass in one sweep: p <- x with the Picard delta
+// statistics (imex_source_map_step.hpp:536-547), and the
 // source_map_eq54_corrected_momentum_field with the physical-boundary
 // pressure (imex_source_map_helpers.hpp:249-268,334-346) and its nonfinite
-// count (:348-357).
-template <int NT>
-__global__ void __launch_bounds__(NT) imex_momentum_kernel(const EcgImexMap m, const double* __restrict__ S,
-                                                           const double* __restrict__ p, const double dt,
-                                                           const double idx, const double idy, double* __restrict__ K,
-                                                           EcgImexStats* __restrict__ st)
-{
-  __shared__ Shared sh;
-  const long long n = static_cast<long long>(m.nx) * m.ny;
-  long long nf = 0;
-  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
-       r += static_cast<long long>(gridDim.x) * NT) {
-    const int j = static_cast<int>(static_cast<unsigned>(r) / static_cast<unsigned>(m.nx)), i = static_cast<int>(r) - j * m.nx;
-    const double gx = 0.5 * (p_b(m, p, i + 1, j) - p_b(m, p, i - 1, j)) * idx;
-    const double gy = 0.5 * (p_b(m, p, i, j + 1) - p_b(m, p, i, j - 1)) * idy;
-    const double k0 = S[r + n] - dt * gx, k1 = S[r + 2 * n] - dt * gy;
-    K[r] = k0;
-    K[r + n] = k1;
-    if (!isfinite(k0) || !isfinite(k1)) ++nf;
-  }
-  ECG_RED_ADD_I(st->k_nonfinite, nf);
-}
-
-// The end of a Picard pass in one sweep: the delta statistics of the new
-// pressure x against the previous p (imex_p_update_kernel) and the eq54
-// momentum from x (imex_momentum_kernel), bit for bit the two kernels in
-// sequence.  x is not copied into p: the caller swaps the two buffers, so x
-// becomes the pass's pressure.
+// count (:348-357), taken from x.  x is not copied into p: the caller swaps
+// the two buffers, so x becomes the pass's pressure.
 template <int NT>
 __global__ void __launch_bounds__(NT) imex_refresh_kernel(const EcgImexMap m, const double* __restrict__ p_old,
                                                           const double* __restrict__ x, const double* __restrict__ S,
@@ -988,11 +986,14 @@ inline cudaError_t imex_faces(const EcgImexMap& m, const double* S, const double
   return cudaGetLastError();
 }
 
-inline cudaError_t imex_rhs(const EcgImexMap& m, const double* S, const double* K, const double* hx, const double* hy,
-                            double dt, double idx, double idy, double* rhs, EcgImexStats* st, cudaStream_t s)
+// faces (mode 0) and right-hand side of a Picard pass in one launch
+inline cudaError_t imex_assemble(const EcgImexMap& m, const double* S, const double* p, const double* K, double* hx,
+                                 double* hy, double dt, double idx, double idy, double* rhs, EcgImexStats* st,
+                                 cudaStream_t s)
 {
-  const long long n = static_cast<long long>(m.nx) * m.ny;
-  imexk::imex_rhs_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, K, hx, hy, dt, idx, idy, rhs, st);
+  const dim3 grid((m.nx + 1 + imexk::AX - 1) / imexk::AX, (m.ny + 1 + imexk::AY - 1) / imexk::AY);
+  imexk::imex_assemble_kernel<imexk::AX * imexk::AY><<<grid, imexk::AX * imexk::AY, 0, s>>>(m, S, p, K, hx, hy, dt, idx,
+                                                                                            idy, rhs, st);
   return cudaGetLastError();
 }
 
@@ -1006,20 +1007,6 @@ inline cudaError_t imex_matrix(const EcgImexMap& m, const double* hx, const doub
   const long long ring = 4LL * (m.nx + m.ny);
   imexk::imex_matrix_edge_kernel<128><<<imexk::blocks_for(n < 2 * ring ? n : ring, 128), 128, 0, s>>>(m, hx, hy, xc,
                                                                                                        yc, st);
-  return cudaGetLastError();
-}
-
-inline cudaError_t imex_p_update(long long n, double* p, const double* x, EcgImexStats* st, cudaStream_t s)
-{
-  imexk::imex_p_update_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(n, p, x, st);
-  return cudaGetLastError();
-}
-
-inline cudaError_t imex_momentum(const EcgImexMap& m, const double* S, const double* p, double dt, double idx,
-                                 double idy, double* K, EcgImexStats* st, cudaStream_t s)
-{
-  const long long n = static_cast<long long>(m.nx) * m.ny;
-  imexk::imex_momentum_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(m, S, p, dt, idx, idy, K, st);
   return cudaGetLastError();
 }
 

@@ -320,7 +320,7 @@ IMEX_CASES = [("gresho_vortex 256x256 periodic, M=0.01", imex_kv(256, 0.01)),
 IMEX_STAR_B, IMEX_PICARD_B, IMEX_CLOSE_B = 88, 80 + 56, 48
 
 
-def imex_leg(dev, stream, steps=3):
+def imex_leg(dev, stream, steps=3, only_case=None):
     """Each IMEX_CASES configuration, IMEX T1/S2 (4 Picard solves, GMRES tol
     1e-10): time per step of the all-FP64 solve and of the FP32-basis /
     FP64-arithmetic solve on the same GPU, their GMRES iterations and solver
@@ -334,7 +334,9 @@ def imex_leg(dev, stream, steps=3):
 
     peak, _ = peaks()
     cases = []
-    for name, kv in IMEX_CASES:
+    for ci, (name, kv) in enumerate(IMEX_CASES):
+        if only_case is not None and ci != only_case:
+            continue
         cfg = read_config(kv).cfg
         cells = cfg.n_cell[0] * cfg.n_cell[1]
         out = {}
@@ -714,6 +716,8 @@ def main():
     ap.add_argument("--slab", action="store_true",
                     help="strong scaling: one grid split over the ranks as x-slabs with an NCCL halo exchange")
     ap.add_argument("--slab-grid", default="10240x2560")
+    ap.add_argument("--imex-case", type=int, default=None,
+                    help="with --only imex: run the IMEX_CASES entry of this index alone")
     ap.add_argument("--only", choices=["imex", "batched", "hllcp"], default=None,
                     help="run one of the extra legs alone (profiling) and print its JSON")
     args = ap.parse_args()
@@ -729,7 +733,8 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         stream = torch.cuda.Stream(device=dev)
-        legs = {"imex": lambda: imex_leg(dev, stream, steps=2), "batched": lambda: batch_leg(dev, stream),
+        legs = {"imex": lambda: imex_leg(dev, stream, steps=2, only_case=args.imex_case),
+                "batched": lambda: batch_leg(dev, stream),
                 "hllcp": lambda: hllcp_leg(dev, stream)}
         leg = legs[args.only]()
         print(json.dumps({"leg": args.only, **leg}))

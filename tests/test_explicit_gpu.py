@@ -17,12 +17,13 @@ CASES = list(golden_io.explicit_cases())
 FAST_TOL = 1e-12
 
 
-# (arith, explicit kernel): exact tile kernel; fast column-strip kernel
-# (default); fast square-tile kernel
-KERNELS = [("exact", 0), ("fast", 0), ("fast", 1)]
+# (arith, explicit kernel): exact tile kernel; fast column-strip kernel with
+# rows staged through shared memory (default); the same with rows loaded into
+# registers; fast square-tile kernel
+KERNELS = [("exact", 0), ("fast", 0), ("fast", 3), ("fast", 1)]
 
 
-@pytest.mark.parametrize("arith,kernel", KERNELS, ids=["exact", "fast-strip", "fast-tile"])
+@pytest.mark.parametrize("arith,kernel", KERNELS, ids=["exact", "fast-strip", "fast-strip-regs", "fast-tile"])
 @pytest.mark.parametrize("key,case", CASES, ids=[k for k, _ in CASES])
 def test_explicit_step_parity(gpu, arith, kernel, key, case):
     cfg = read_config(golden_io.kv_of(case["kv"])).cfg

@@ -124,9 +124,11 @@ PROBLEMS = [("gresho_vortex", "hllc"), ("toro1", "xie_am_hllc_p"), ("shock_densi
             ("advection_blob", "lowmach_hllc")]
 
 
-# tile_y selects the explicit kernel: 0 column strips with paired faces, 2
-# column strips with faces one at a time, 1 square 16x16 tiles, 8 the 32x8 tiles
-@pytest.mark.parametrize("tile_y", [0, 1, 2, 8])
+# tile_y selects the explicit kernel: 0 column strips with paired faces and
+# rows staged through shared memory, 3 the same with rows loaded into
+# registers, 2 column strips with faces one at a time, 1 square 16x16 tiles, 8
+# the 32x8 tiles
+@pytest.mark.parametrize("tile_y", [0, 1, 2, 3, 8])
 @pytest.mark.parametrize("arith", ["exact", "fast"])
 @pytest.mark.parametrize("problem,riemann", PROBLEMS)
 def test_noalloc_larger_grid(gpu, arith, problem, riemann, tile_y):
