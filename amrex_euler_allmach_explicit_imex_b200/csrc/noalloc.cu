@@ -152,17 +152,6 @@ ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gp
     set_err(err, err_len, "layout does not cover [0, nx) x [0, ny)");
     return ECG_ERR_BAD_ARG;
   }
-  // The step reads neighbour cells of state_in while it writes state_out, so
-  // the two arrays (4 planes of nstride doubles from their Array4 bases) must
-  // not share a byte.
-  {
-    const auto a0 = reinterpret_cast<uintptr_t>(state_in), b0 = reinterpret_cast<uintptr_t>(state_out);
-    const uintptr_t len = sizeof(double) * 4 * static_cast<uintptr_t>(nstride);
-    if (a0 < b0 + len && b0 < a0 + len) {
-      set_err(err, err_len, "state_in and state_out overlap");
-      return ECG_ERR_BAD_ARG;
-    }
-  }
   ecg_gpu_options o;
   if (opt) o = *opt;
   else ecg_default_gpu_options(&o);
@@ -182,6 +171,17 @@ ecg_status ecg_euler_fv_one_step_noalloc(const ecg_run_config* cfg, const ecg_gp
     return ECG_ERR_BAD_ARG;
   }
 
+  // The step reads neighbour cells of state_in while it writes state_out, so
+  // the two arrays (4 planes of nstride doubles from their Array4 bases) must
+  // not share a byte.
+  {
+    const auto a0 = reinterpret_cast<uintptr_t>(state_in), b0 = reinterpret_cast<uintptr_t>(state_out);
+    const uintptr_t len = sizeof(double) * 4 * static_cast<uintptr_t>(nstride);
+    if (a0 < b0 + len && b0 < a0 + len) {
+      set_err(err, err_len, "state_in and state_out overlap");
+      return ECG_ERR_BAD_ARG;
+    }
+  }
   DeviceGuard guard;
   cudaError_t e = guard.enter(o.device);
   if (e != cudaSuccess) return fail(err, err_len, ECG_ERR_NO_DEVICE, "select device", e);

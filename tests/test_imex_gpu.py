@@ -39,20 +39,30 @@ def test_imex_step_fp64(gpu, name, arith):
         assert d.solver_status == ref_status, api.solver_status_str(d.solver_status)
     assert d.picard_pressure_solves_used == int(c["d_picard_pressure_solves_used"])
     # GMRES with classical Gram-Schmidt + reorthogonalisation vs the reference's
-    # modified Gram-Schmidt: iteration counts agree to rounding except on
-    # near-singular systems (the reflecting 1D Sod row), so allow 20 %.
+    # modified Gram-Schmidt: on the 2D systems the four solves' iteration
+    # counts agree to one each.  The reflecting 1D Sod row is nearly singular:
+    # its count follows the last bits of the Picard iterate, so 20 % there.
+    near_singular = name == "sod_reflect"
     ref_its = int(c["d_solver_iterations"])
-    assert abs(d.solver_iterations - ref_its) <= max(cfg.imex_picard_iterations, 0.2 * ref_its)
+    slack = max(cfg.imex_picard_iterations, 0.2 * ref_its) if near_singular else cfg.imex_picard_iterations
+    assert abs(d.solver_iterations - ref_its) <= slack
     assert golden_io.state_rel_err(u1, c["u1"]) <= 1e-9
     assert d.pressure_linear_residual_relative_linf <= cfg.imex_solver_tol or d.pressure_linear_residual_linf <= cfg.imex_solver_tol
     assert d.pressure_matrix_rows == int(c["d_pressure_matrix_rows"])
-    # A coefficient such as -yc*(hn - hs) is dropped when it is exactly zero.
-    # On the x-only Sod data every row of the 4-row grid carries the same face
-    # enthalpies up to rounding, so whether hn - hs is exactly zero follows
-    # the last bit of the Picard iterate: allow 10 % (the 1D row loses at most
-    # two of its eight entries).
-    assert abs(d.pressure_matrix_nonzeros - int(c["d_pressure_matrix_nonzeros"])) <= 0.1 * int(c["d_pressure_matrix_nonzeros"])
-    assert abs(d.pressure_matrix_max_row_width - int(c["d_pressure_matrix_max_row_width"])) <= 1  # same cause
+    if near_singular:
+        # A coefficient such as -yc*(hn - hs) is dropped when it is exactly
+        # zero.  On the x-only Sod data every row of the 4-row grid carries
+        # the same face enthalpies up to rounding, so whether hn - hs is
+        # exactly zero follows the last bit of the Picard iterate: allow 10 %
+        # (the 1D row loses at most two of its eight entries).
+        assert abs(d.pressure_matrix_nonzeros - int(c["d_pressure_matrix_nonzeros"])) <= 0.1 * int(c["d_pressure_matrix_nonzeros"])
+        assert abs(d.pressure_matrix_max_row_width - int(c["d_pressure_matrix_max_row_width"])) <= 1
+    else:
+        # exact zeros of enthalpy differences in the uniform parts of the
+        # state follow the last bits of the iterate as well, but rarely
+        ref_nnz = int(c["d_pressure_matrix_nonzeros"])
+        assert abs(d.pressure_matrix_nonzeros - ref_nnz) <= 0.01 * ref_nnz
+        assert abs(d.pressure_matrix_max_row_width - int(c["d_pressure_matrix_max_row_width"])) <= 1
     for f in ["kinetic_jacobian_abs_max", "pressure_energy_residual_before_linf", "rho_min", "pressure_min",
               "internal_energy_min", "solved_pressure_min", "solved_pressure_max", "energy_flux_linf",
               "momentum_correction_linf", "energy_correction_linf", "eq78_divergence_linf"]:
