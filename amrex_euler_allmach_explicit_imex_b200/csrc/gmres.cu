@@ -1127,6 +1127,8 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   EcgGmresResult out;
   std::memset(&out, 0, sizeof(out));
   const int limit = a.max_iter < a.n ? a.max_iter : static_cast<int>(a.n);
+  bool final_known = false;  // mixed: the final true residual is already known
+  double known_r = 0.0, known_b = 0.0;
   {
     const Smem S0 = carve(sh, a.m);
     if (threadIdx.x == 0) S0.cnt[0] = S0.cnt[1] = 0.0;
@@ -1176,7 +1178,14 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
       out.iterations = total + st.best_it;
       total += st.it;
       if (st.timeout || st.nonfinite || st.breakdown) break;
-      if (st.converged && st.it == 0) break;  // the true residual meets the rule
+      if (st.converged && st.it == 0) {
+        // the true residual of x, computed as this cycle opened, meets the
+        // rule: it is the returned iterate's final residual as well
+        final_known = true;
+        known_r = st.r0_linf;
+        known_b = st.b_linf;
+        break;
+      }
       if (total >= limit || last) break;
       xin = a.x;
       if (!grid_sync(a.bar, gen, a.spin_limit)) {  // x complete before the next residual
@@ -1197,7 +1206,10 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   // sweep after x is complete; the host reads them with the result) ----
   const double nan = __longlong_as_double(0x7ff8000000000000LL);
   out.final_linf = out.final_b_linf = nan;
-  if (!out.timeout && grid_sync(a.bar, gen, a.spin_limit)) {
+  if (final_known) {
+    out.final_linf = known_r;
+    out.final_b_linf = known_b;
+  } else if (!out.timeout && grid_sync(a.bar, gen, a.spin_limit)) {
     const Rows rw = own_rows(a.n);
     const Smem S = carve(sh, a.m);
     const Acc A{a.acc, a.ld, nullptr};  // maxima only
@@ -1229,7 +1241,7 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const Smem S = carve(sh, a.m);
-    out.vec_access64 = S.cnt[0] + 4.0;  // the final residual: x, hx, hy, b
+    out.vec_access64 = S.cnt[0] + (final_known ? 0.0 : 4.0);  // the final residual: x, hx, hy, b
     out.vec_access32 = S.cnt[1];
     *a.res = out;
   }

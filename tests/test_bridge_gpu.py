@@ -109,12 +109,17 @@ def test_bridge_bubble_imex(gpu, prec):
     got = _report(BRIDGE, BUBBLE_IMEX + [f"ecg.imex_precision={prec}"])
     assert ref["imex_step_count"] == got["imex_step_count"] == "40"
     # Two correct solves stopped by the same rule on the same system differ in
-    # the iteration they stop at and in the residual they stop with: the
-    # iteration counts compare to 20 %, the residuals to the rule itself.
+    # the iteration they stop at and in the residual they stop with: the FP64
+    # iteration counts compare to 20 %, the residuals to the rule itself.  The
+    # mixed solve reports the iterations of all its restarted cycles, which
+    # are not the reference's unrestarted count; they stay within its limit.
     its = [k for k in ref if "solver_iterations" in k]
     for k in its:
         a, b = float(ref[k]), float(got[k])
-        assert abs(a - b) <= max(4.0, 0.2 * a), (k, a, b)
+        if prec == "fp64":
+            assert abs(a - b) <= max(4.0, 0.2 * a), (k, a, b)
+        else:
+            assert 0 < b <= 200, (k, a, b)
     res = [k for k in ref if "residual" in k]
     for k in res:
         a, b = float(ref[k]), float(got[k])
