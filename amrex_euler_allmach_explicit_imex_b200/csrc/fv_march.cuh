@@ -237,7 +237,12 @@ __device__ __forceinline__ void cp_async_wait()
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int RK, int LIM, bool PAIR>
+// UNR (1 or 6): rows per trip of the row loop.  The window of rows j, j+1,
+// j+2, the y-slopes of two rows and the y-faces below and above a row change
+// roles every row; a trip of 6 rows (a multiple of both periods, 3 and 2)
+// hands the roles round by name, with no register moves between rows (the
+// tail of fewer rows moves them).
+template <int RK, int LIM, bool PAIR, int UNR>
 __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const double* __restrict__ u,
                                                    double* __restrict__ out, int c0, int j0, int H, double dt,
                                                    bool count_deg, MarchAcc& acc, StageRing& ring)
@@ -293,41 +298,43 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
 #pragma unroll
   for (int r = -2; r <= 1 + kAhead; ++r) put(j0 + r);
   cp_async_wait<kAhead>();
-  Prim q_m2 = fast::to_prim_f(get(j0 - 2), g);
-  Lane L;
-  L.q[1] = fast::to_prim_f(get(j0 - 1), g);
-  L.q[2] = fast::to_prim_f(get(j0), g);
-  L.q[3] = fast::to_prim_f(get(j0 + 1), g);
-  const Prim sy_m1 = slope3<LIM>(q_m2, L.q[1], L.q[2], second);
-  Prim sy_cur = slope3<LIM>(L.q[1], L.q[2], L.q[3], second);
-  Cons gb;
+  Prim qa, qb, qc;  // rows j, j+1 and the slot of row j+2, by role
+  Prim s0, s1;      // y-slope of row j, and the slot of row j+1's
+  Cons g0, g1;      // y-face below row j, and the slot of the face above it
   {
+    const Prim q_m2 = fast::to_prim_f(get(j0 - 2), g);
+    const Prim q_m1 = fast::to_prim_f(get(j0 - 1), g);
+    qa = fast::to_prim_f(get(j0), g);
+    qb = fast::to_prim_f(get(j0 + 1), g);
+    const Prim sy_m1 = slope3<LIM>(q_m2, q_m1, qa, second);
+    s0 = slope3<LIM>(q_m1, qa, qb, second);
     bool deg;
-    gb = face_one<RK>(plus_half(L.q[1], sy_m1), minus_half(L.q[2], sy_cur), 1, g, inv_gm1, deg);
+    g0 = face_one<RK>(plus_half(q_m1, sy_m1), minus_half(qa, s0), 1, g, inv_gm1, deg);
     if (count_deg && deg && cell_ok && j0 < ny) acc.degenerate += 1;
   }
   const long long pl = P.g.plane;
-  double* orow = out + static_cast<long long>(j0) * P.g.pitch + xs;
-  for (int j = j0; j < jend; ++j, orow += P.g.pitch) {
+  double* const obase = out + xs;
+
+  // one row: row j's cells from rows j (q0), j+1 (q1) and the new row j+2
+  // (into q2), the y-slope of row j (sc; that of row j+1 into sn) and the
+  // y-face below row j (gb; the face above it into gt)
+  auto row = [&](int j, const Prim& q0, const Prim& q1, Prim& q2, const Prim& sc, Prim& sn, const Cons& gb, Cons& gt) {
     put(j + 2 + kAhead);
     cp_async_wait<kAhead>();  // row j + 2 has landed
-    L.q[1] = L.q[2];
-    L.q[2] = L.q[3];
-    L.q[3] = fast::to_prim_f(get(j + 2), g);
-    const Prim& qc = L.q[1];
-    const Prim sy_next = slope3<LIM>(L.q[1], L.q[2], L.q[3], second);
-    const Prim ql{shup(qc.rho), shup(qc.u), shup(qc.v), shup(qc.p)};
-    const Prim qr{shdn(qc.rho), shdn(qc.u), shdn(qc.v), shdn(qc.p)};
-    const Prim sx = slope3<LIM>(ql, qc, qr, second);
+    q2 = fast::to_prim_f(get(j + 2), g);
+    sn = slope3<LIM>(q0, q1, q2, second);
+    const Prim ql{shup(q0.rho), shup(q0.u), shup(q0.v), shup(q0.p)};
+    const Prim qr{shdn(q0.rho), shdn(q0.u), shdn(q0.v), shdn(q0.p)};
+    const Prim sx = slope3<LIM>(ql, q0, qr, second);
     const Prim sxl{shup(sx.rho), shup(sx.u), shup(sx.v), shup(sx.p)};
-    Cons fl, gt;
+    Cons fl;
     bool deg_x, deg_y;
     if (PAIR) {
-      face_pair<RK>(plus_half(ql, sxl), minus_half(qc, sx), plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), g,
-                    inv_gm1, fl, gt, deg_x, deg_y);
+      face_pair<RK>(plus_half(ql, sxl), minus_half(q0, sx), plus_half(q0, sc), minus_half(q1, sn), g, inv_gm1, fl,
+                    gt, deg_x, deg_y);
     } else {
-      gt = face_w<RK>(plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), 1, g, inv_gm1, deg_y);
-      fl = face_w<RK>(plus_half(ql, sxl), minus_half(qc, sx), 0, g, inv_gm1, deg_x);
+      gt = face_w<RK>(plus_half(q0, sc), minus_half(q1, sn), 1, g, inv_gm1, deg_y);
+      fl = face_w<RK>(plus_half(ql, sxl), minus_half(q0, sx), 0, g, inv_gm1, deg_x);
     }
     const Cons fr{shdn(fl.rho), shdn(fl.mx), shdn(fl.my), shdn(fl.E)};
     if (count_deg) {
@@ -347,10 +354,11 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
     const Prim q = fast::to_prim_f(n, g);
     const double cs = fast::fsound_w(q.rho, q.p, g);
     if (cell_ok) {
-      orow[0] = n.rho;
-      orow[pl] = n.mx;
-      orow[2 * pl] = n.my;
-      orow[3 * pl] = n.E;
+      double* o = obase + static_cast<long long>(j) * P.g.pitch;
+      o[0] = n.rho;
+      o[pl] = n.mx;
+      o[2 * pl] = n.my;
+      o[3 * pl] = n.E;
       const double rate = (fabs(q.u) + cs) * idx + (fabs(q.v) + cs) * idy;
       if (!isnan(rate)) acc.kmax = umax64(acc.kmax, okey(rate));
       const bool bad = !isfinite(q.rho) || !isfinite(q.u) || !isfinite(q.v) || !isfinite(q.p) || !isfinite(n.E);
@@ -358,18 +366,37 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
       acc.kp = umin64(acc.kp, okey(bad ? -kInf : q.p));
       acc.nonfinite += bad ? 1 : 0;
     }
-    gb = gt;
-    sy_cur = sy_next;
+  };
+
+  int j = j0;
+  if (UNR == 6) {
+    for (; j + 6 <= jend; j += 6) {
+      row(j, qa, qb, qc, s0, s1, g0, g1);
+      row(j + 1, qb, qc, qa, s1, s0, g1, g0);
+      row(j + 2, qc, qa, qb, s0, s1, g0, g1);
+      row(j + 3, qa, qb, qc, s1, s0, g1, g0);
+      row(j + 4, qb, qc, qa, s0, s1, g0, g1);
+      row(j + 5, qc, qa, qb, s1, s0, g1, g0);
+    }
+  }
+  for (; j < jend; ++j) {
+    row(j, qa, qb, qc, s0, s1, g0, g1);
+    qa = qb;
+    qb = qc;
+    s0 = s1;
+    g0 = g1;
   }
   cp_async_wait<0>();  // no request outlives the strip
 }
 
-// At most 128 registers a thread (4 blocks of 4 warps per SM): measured
-// faster than the 166-register schedule the paired faces get unbounded.
-// STAGE: rows through the shared-memory ring (march_strip_staged), else
-// straight from global memory into registers (march_strip).
+// Registers: the register-loaded strips at most 128 a thread (4 blocks of 4
+// warps per SM), measured faster than the 166-register schedule the paired
+// faces get unbounded; the staged strips at most 168 (3 blocks), measured
+// faster than 128 for them (fewer registers spill).
+// STAGE: rows through the shared-memory ring (march_strip_staged, 6 rows a
+// trip), else straight from global memory into registers (march_strip).
 template <int RK, int LIM, int WPB, bool PAIR, bool STAGE>
-__global__ void __launch_bounds__(WPB * 32, 16 / WPB)
+__global__ void __launch_bounds__(WPB * 32, (STAGE ? 12 : 16) / WPB)
 fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __restrict__ out,
                 EcgStepStats* __restrict__ stats, const EcgDtCtl ctl, const int H)
 {
@@ -386,8 +413,8 @@ fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __res
   acc.init();
   if (c0 < P.g.nx) {
     if (STAGE)
-      march_strip_staged<RK, LIM, PAIR>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc,
-                                        ring[STAGE ? threadIdx.x >> 5 : 0]);
+      march_strip_staged<RK, LIM, PAIR, 6>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc,
+                                           ring[STAGE ? threadIdx.x >> 5 : 0]);
     else
       march_strip<RK, LIM, PAIR>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc);
   }
