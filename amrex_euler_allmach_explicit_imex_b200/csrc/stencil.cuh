@@ -488,13 +488,13 @@ cudaError_t launch_fv_step(const EcgFvParams& p, const double* in, double* out, 
                            const EcgDtCtl& ctl, int tile_y, cudaStream_t s)
 {
 #ifdef ECG_FAST_KERNEL
-  // 0: column-strip kernel, x- and y-faces evaluated together, rows loaded
-  // into registers (default); 3: the same with rows staged through shared
-  // memory by cp.async (bit-identical, measured 2.6 % slower: the load
-  // latency is not what binds this kernel); 2: column-strip kernel, faces one
-  // after the other; 1: square-tile kernel
-  if (tile_y == 0) return march::launch(p, in, out, stats, ctl, s, true, false);
-  if (tile_y == 3) return march::launch(p, in, out, stats, ctl, s, true, true);
+  // 0: column-strip kernel, x- and y-faces evaluated together, rows staged
+  // through shared memory by cp.async, 168 registers (default: 75.8 us at
+  // 2560x640); 3: the same with rows loaded into registers, 128 registers
+  // (77.8 us); 2: column-strip kernel, faces one after the other; 1:
+  // square-tile kernel
+  if (tile_y == 0) return march::launch(p, in, out, stats, ctl, s, true, true);
+  if (tile_y == 3) return march::launch(p, in, out, stats, ctl, s, true, false);
   if (tile_y == 2) return march::launch(p, in, out, stats, ctl, s, false, false);
   if (tile_y == 1) return fast::launch(p, in, out, stats, ctl, s);
 #endif

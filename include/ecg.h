@@ -151,10 +151,10 @@ typedef struct ecg_gpu_options {
   int32_t mixed_max_refinements; /* mixed: cycles, each opened with the true FP64 residual */
   int32_t tile_x;           /* column-strip kernel: rows each warp marches (0: sized so the grid fills one wave) */
   int32_t tile_y;           /* explicit kernel: 0 default (column strips, x- and y-faces
-                               evaluated together, rows loaded into registers), 3 the same
-                               with rows staged through shared memory by cp.async, 2 column
-                               strips with faces one at a time, 1 square 16x16 tiles, 8 or
-                               16 the 32 x tile_y tiles */
+                               evaluated together, rows staged through shared memory by
+                               cp.async), 3 the same with rows loaded into registers, 2
+                               column strips with faces one at a time, 1 square 16x16
+                               tiles, 8 or 16 the 32 x tile_y tiles */
   int32_t mixed_reorth;     /* mixed: Gram-Schmidt second pass (DGKS) of the FP32-basis cycles:
                                1 when ||w'|| < ||w||/sqrt(2), as the FP64 solve; 0 (default) only
                                when ||w'|| < 1e-3 ||w||, where the Pythagorean norm would lose digits */

@@ -18,12 +18,12 @@ FAST_TOL = 1e-12
 
 
 # (arith, explicit kernel): exact tile kernel; fast column-strip kernel with
-# rows loaded into registers (default); the same with rows staged through
-# shared memory; fast square-tile kernel
+# rows staged through shared memory (default); the same with rows loaded into
+# registers; fast square-tile kernel
 KERNELS = [("exact", 0), ("fast", 0), ("fast", 3), ("fast", 1)]
 
 
-@pytest.mark.parametrize("arith,kernel", KERNELS, ids=["exact", "fast-strip", "fast-strip-staged", "fast-tile"])
+@pytest.mark.parametrize("arith,kernel", KERNELS, ids=["exact", "fast-strip", "fast-strip-regs", "fast-tile"])
 @pytest.mark.parametrize("key,case", CASES, ids=[k for k, _ in CASES])
 def test_explicit_step_parity(gpu, arith, kernel, key, case):
     cfg = read_config(golden_io.kv_of(case["kv"])).cfg

@@ -125,8 +125,8 @@ PROBLEMS = [("gresho_vortex", "hllc"), ("toro1", "xie_am_hllc_p"), ("shock_densi
 
 
 # tile_y selects the explicit kernel: 0 column strips with paired faces and
-# rows loaded into registers, 3 the same with rows staged through shared
-# memory, 2 column strips with faces one at a time, 1 square 16x16 tiles, 8
+# rows staged through shared memory, 3 the same with rows loaded into
+# registers, 2 column strips with faces one at a time, 1 square 16x16 tiles, 8
 # the 32x8 tiles
 @pytest.mark.parametrize("tile_y", [0, 1, 2, 3, 8])
 @pytest.mark.parametrize("arith", ["exact", "fast"])
