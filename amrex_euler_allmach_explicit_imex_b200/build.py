@@ -37,6 +37,7 @@ SOURCES = {
     "batched.cu": ["-fmad=true"],
     "adjoint.cu": ["-fmad=true"],
     "noalloc.cu": [],
+    "hoststage.cu": [],
     "peak.cu": [],
     "output.cu": ["-fmad=false"],
     "paper.cu": ["-fmad=false"],

@@ -251,6 +251,8 @@ ecg_ctx::~ecg_ctx()
   cudaFreeHost(h_state_stats);
   for (cudaEvent_t e : band_up) cudaEventDestroy(e);
   for (cudaEvent_t e : band_done) cudaEventDestroy(e);
+  for (cudaEvent_t e : band_dl) cudaEventDestroy(e);
+  host_stage_destroy(stage);
   if (up_stream) cudaStreamDestroy(up_stream);
   if (down_stream) cudaStreamDestroy(down_stream);
   if (own_stream && stream) cudaStreamDestroy(stream);
@@ -436,6 +438,71 @@ ecg_status ecg_synchronize(ecg_ctx* c)
 
 // ---- state exchange ----------------------------------------------------------
 
+// One event per band of rows in `ev` (created on first use).
+static bool band_events(ecg_ctx* c, std::vector<cudaEvent_t>& ev, int nb)
+{
+  while (static_cast<int>(ev.size()) < nb) {
+    cudaEvent_t e = nullptr;
+    if (!cuda_ok(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) return false;
+    ev.push_back(e);
+  }
+  return true;
+}
+
+// Rows [r0, r1) of the 4 planes between the compact stage (pitch nx) and the
+// device state (the context's pitch and plane).
+static cudaError_t stage_rows(ecg_ctx* c, double* stage, double* dev, int r0, int r1, bool upload, cudaStream_t st)
+{
+  const int nx = c->grid.nx;
+  const size_t splane = static_cast<size_t>(nx) * static_cast<size_t>(c->grid.ny);
+  for (int n = 0; n < 4; ++n) {
+    double* s = stage + n * splane + static_cast<size_t>(r0) * nx;
+    double* d = dev + n * c->grid.plane + static_cast<long long>(r0) * c->grid.pitch;
+    const cudaError_t e =
+        upload ? cudaMemcpy2DAsync(d, sizeof(double) * c->grid.pitch, s, sizeof(double) * nx, sizeof(double) * nx,
+                                   r1 - r0, cudaMemcpyHostToDevice, st)
+               : cudaMemcpy2DAsync(s, sizeof(double) * nx, d, sizeof(double) * c->grid.pitch, sizeof(double) * nx,
+                                   r1 - r0, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// The state to or from a pageable host box (host: offset to cell (0, 0))
+// through the pinned stage in bands of rows: the host threads copy band b+1
+// while band b crosses.
+static ecg_status transfer_staged(ecg_ctx* c, double* host, int64_t jstride, int64_t nstride, bool upload)
+{
+  const int nx = c->grid.nx, ny = c->grid.ny;
+  HostStage* hs = host_stage(c);
+  if (!hs) return ECG_ERR_CUDA;
+  const int nb = ny < 64 ? 1 : std::min(8, ny / 32);
+  auto row0 = [&](int b) { return static_cast<int>(static_cast<long long>(ny) * b / nb); };
+  double* dev = c->cur_state_mut();
+  if (upload) {
+    double* stage = host_stage_in(hs);
+    for (int b = 0; b < nb; ++b) {
+      host_stage_copy(hs, stage, host, jstride, nstride, nx, ny, row0(b), row0(b + 1), true);
+      if (!cuda_ok(c, stage_rows(c, stage, dev, row0(b), row0(b + 1), true, c->stream), "upload")) return ECG_ERR_CUDA;
+    }
+    c->uploaded = true;
+    c->invalidate();
+    return cuda_ok(c, cudaStreamSynchronize(c->stream), "sync") ? ECG_OK : ECG_ERR_CUDA;
+  }
+  double* stage = host_stage_out(hs);
+  if (!band_events(c, c->band_dl, nb)) return ECG_ERR_CUDA;
+  for (int b = 0; b < nb; ++b) {
+    if (!cuda_ok(c, stage_rows(c, stage, dev, row0(b), row0(b + 1), false, c->stream), "download") ||
+        !cuda_ok(c, cudaEventRecord(c->band_dl[b], c->stream), "event"))
+      return ECG_ERR_CUDA;
+  }
+  for (int b = 0; b < nb; ++b) {
+    if (!cuda_ok(c, cudaEventSynchronize(c->band_dl[b]), "sync")) return ECG_ERR_CUDA;
+    host_stage_copy(hs, stage, host, jstride, nstride, nx, ny, row0(b), row0(b + 1), false);
+  }
+  return ECG_OK;
+}
+
 static ecg_status transfer(ecg_ctx* c, double* host, const double* hostc, int32_t lo_x, int32_t lo_y, int64_t jstride,
                            int64_t nstride, bool upload, bool device_side)
 {
@@ -446,6 +513,8 @@ static ecg_status transfer(ecg_ctx* c, double* host, const double* hostc, int32_
   const cudaMemcpyKind kind = device_side ? cudaMemcpyDeviceToDevice
                                           : (upload ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost);
   double* dev = upload ? c->cur_state_mut() : c->cur_state_mut();
+  if (!device_side && host_pageable(upload ? static_cast<const void*>(hostc) : static_cast<const void*>(host)))
+    return transfer_staged(c, upload ? const_cast<double*>(hostc) + off : host + off, jstride, nstride, upload);
   for (int n = 0; n < 4; ++n) {
     double* d = dev + n * c->grid.plane;
     cudaError_t e;
@@ -606,13 +675,20 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
   if (!cuda_ok(c, cudaEventRecord(c->band_done[0], c->stream), "event") ||
       !cuda_ok(c, cudaStreamWaitEvent(c->up_stream, c->band_done[0], 0), "event"))
     return ECG_ERR_CUDA;
+  // Pageable boxes cross through the context's pinned stage (compact, pitch
+  // nx): the host threads copy band b+1 into it while band b crosses, and the
+  // downloaded bands are copied out of it as each one lands.
+  const bool stage_in = host_pageable(in), stage_out = host_pageable(out);
+  HostStage* hs = nullptr;
+  if ((stage_in || stage_out) && !(hs = host_stage(c))) return ECG_ERR_CUDA;
+  if (stage_out && !band_events(c, c->band_dl, nb)) return ECG_ERR_CUDA;
+  const long long splane = static_cast<long long>(nx) * ny;
   // The four field planes of a band move in one 3D copy (planes at a fixed
   // stride on both sides); per-plane 2D copies otherwise.  Fewer, larger copy
   // commands let the two directions share the link better.
-  const bool planes3d = nstride % jstride == 0 && c->grid.plane % c->grid.pitch == 0;
   auto copy_band = [&](double* dst, long long dpitch, long long dslice, const double* src, long long spitch,
                        long long sslice, int rows, cudaMemcpyKind kind, cudaStream_t st) -> cudaError_t {
-    if (planes3d) {
+    if (sslice % spitch == 0 && dslice % dpitch == 0) {
       cudaMemcpy3DParms m;
       std::memset(&m, 0, sizeof(m));
       m.srcPtr = make_cudaPitchedPtr(const_cast<double*>(src), sizeof(double) * spitch, sizeof(double) * nx,
@@ -632,11 +708,19 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
   };
   for (int b = 0; b < nb; ++b) {
     const int r0 = row0(b), r1 = row0(b + 1);
-    if (!cuda_ok(c, copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
-                              in + off + static_cast<int64_t>(r0) * jstride, jstride, nstride, r1 - r0,
-                              cudaMemcpyHostToDevice, c->up_stream),
-                 "upload band"))
-      return ECG_ERR_CUDA;
+    cudaError_t e;
+    if (stage_in) {
+      double* stage = host_stage_in(hs);
+      host_stage_copy(hs, stage, const_cast<double*>(in) + off, jstride, nstride, nx, ny, r0, r1, true);
+      e = copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
+                    stage + static_cast<long long>(r0) * nx, nx, splane, r1 - r0, cudaMemcpyHostToDevice,
+                    c->up_stream);
+    } else {
+      e = copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
+                    in + off + static_cast<int64_t>(r0) * jstride, jstride, nstride, r1 - r0, cudaMemcpyHostToDevice,
+                    c->up_stream);
+    }
+    if (!cuda_ok(c, e, "upload band")) return ECG_ERR_CUDA;
     if (!cuda_ok(c, cudaEventRecord(c->band_up[b], c->up_stream), "event")) return ECG_ERR_CUDA;
   }
   c->uploaded = true;
@@ -666,11 +750,25 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
         !cuda_ok(c, cudaStreamWaitEvent(c->down_stream, c->band_done[b], 0), "event"))
       return ECG_ERR_CUDA;
     const int r0 = row0(b), r1 = row0(b + 1);
-    if (!cuda_ok(c, copy_band(out + off + static_cast<int64_t>(r0) * jstride, jstride, nstride,
-                              nxt + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane, r1 - r0,
-                              cudaMemcpyDeviceToHost, c->down_stream),
-                 "download band"))
+    if (stage_out) {
+      if (!cuda_ok(c, copy_band(host_stage_out(hs) + static_cast<long long>(r0) * nx, nx, splane,
+                                nxt + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
+                                r1 - r0, cudaMemcpyDeviceToHost, c->down_stream),
+                   "download band") ||
+          !cuda_ok(c, cudaEventRecord(c->band_dl[b], c->down_stream), "event"))
+        return ECG_ERR_CUDA;
+    } else if (!cuda_ok(c, copy_band(out + off + static_cast<int64_t>(r0) * jstride, jstride, nstride,
+                                     nxt + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
+                                     r1 - r0, cudaMemcpyDeviceToHost, c->down_stream),
+                        "download band")) {
       return ECG_ERR_CUDA;
+    }
+  }
+  if (stage_out) {
+    for (int b = 0; b < nb; ++b) {
+      if (!cuda_ok(c, cudaEventSynchronize(c->band_dl[b]), "sync")) return ECG_ERR_CUDA;
+      host_stage_copy(hs, host_stage_out(hs), out + off, jstride, nstride, nx, ny, row0(b), row0(b + 1), false);
+    }
   }
   c->cur ^= 1;
   ++c->host_step;

@@ -11,6 +11,7 @@
 
 struct EcgImexState;  // imex.cu
 struct EcgOutput;     // output.cu
+struct HostStage;     // hoststage.cu
 
 struct ecg_ctx {
   static constexpr int kChunk = 32;  // explicit steps per captured graph
@@ -27,7 +28,10 @@ struct ecg_ctx {
   // pipelined host step (ecg_euler_fv_one_step_host): copy streams and one
   // event per band for the upload and for the step
   cudaStream_t up_stream = nullptr, down_stream = nullptr;
-  std::vector<cudaEvent_t> band_up, band_done;
+  std::vector<cudaEvent_t> band_up, band_done, band_dl;
+  // pageable host boxes: pinned staging copies of the state and the host
+  // threads that fill and drain them (hoststage.cu), made on first use
+  HostStage* stage = nullptr;
 
   double* d_state[2] = {nullptr, nullptr};  // double buffer, 4 planes each
   int cur = 0;
@@ -95,6 +99,18 @@ bool is_bubble(const ecg_run_config& c);
 bool reduce_state(ecg_ctx* c);
 bool fetch_fused(ecg_ctx* c);
 }  // namespace ecgi
+
+// hoststage.cu: copies between pageable host boxes and the device through
+// the context's pinned staging buffers
+bool host_pageable(const void* p);
+HostStage* host_stage(ecg_ctx* c);  // null when the pinned buffers cannot be allocated (c->err set)
+void host_stage_destroy(HostStage* s);
+double* host_stage_in(HostStage* s);
+double* host_stage_out(HostStage* s);
+// rows [r0, r1) of the 4 planes between the caller's box (offset to cell (0, 0))
+// and the compact stage, on the staging threads
+void host_stage_copy(HostStage* s, double* stage, double* host, int64_t jstride, int64_t nstride, int nx, int ny,
+                     int r0, int r1, bool to_stage);
 
 // imex.cu
 void imex_free(ecg_ctx* c);

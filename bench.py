@@ -646,8 +646,9 @@ def run_ours(args):
     e2e_value = sum_over_ranks(dist, cells * e2e_k, dev) / (e2e_ms * 1e-3)
 
     # The same calls on pageable host memory (an FArrayBox as AMReX allocates
-    # it, never registered with CUDA): the copies then go through the
-    # driver's staging buffers.
+    # it, never registered with CUDA): the library copies each band through
+    # its own pinned stage on host threads while the previous band crosses
+    # (the first call allocates the stage; the warm-up calls cover it).
     page_a = np.ascontiguousarray(host_a.numpy()).copy()
     page_b = np.empty_like(page_a)
     for _ in range(2):

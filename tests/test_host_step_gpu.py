@@ -62,3 +62,57 @@ def test_host_step_in_place(gpu):
         ctx.upload(ref)
         api.euler_fv_one_step_host(ctx, u, u, dt)
         assert golden_io.state_rel_err(u, want) <= 1e-12
+
+
+def _pinned(shape):
+    import torch
+
+    return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+
+
+def _padded(u, g, extra):
+    """u inside a ghost-padded box: lo = -g, rows nx + 2g + extra long,
+    planes one row apart more than the box needs."""
+    _, ny, nx = u.shape
+    js = nx + 2 * g + extra
+    ns = js * (ny + 2 * g + 1)
+    buf = np.full(4 * ns, np.nan)
+    box = np.lib.stride_tricks.as_strided(buf[g * js + g:], shape=u.shape, strides=(8 * ns, 8 * js, 8))
+    box[...] = u
+    return buf, box, js, ns
+
+
+@pytest.mark.parametrize("name", ["bubble", "toro_periodic_y"])
+def test_pageable_boxes_cross_like_pinned_ones(gpu, name):
+    """Pageable host boxes go through the library's pinned stage in bands of
+    rows; the bits that cross are those of a pinned box, and a ghost-padded
+    Array4 box (lo = -2, padded rows and planes) keeps its ghosts."""
+    from amrex_euler_allmach_explicit_imex_b200._lib import check, load
+
+    lib = load()
+    cfg = read_config(CASES[name]).cfg
+    with api.Context(cfg) as ctx:
+        api.initialize_state(ctx)
+        u0 = ctx.download(_pinned((4, ctx.ny, ctx.nx)))
+        dt = api.compute_euler_dt(ctx)
+        pin_out = _pinned(u0.shape)
+        api.euler_fv_one_step_host(ctx, u0, pin_out, dt)
+        page_out = np.empty_like(u0)
+        api.euler_fv_one_step_host(ctx, np.array(u0), page_out, dt)
+        np.testing.assert_array_equal(page_out, pin_out)
+        # a padded pageable box: upload, host step in place, download
+        g = 2
+        buf, box, js, ns = _padded(u0, g, 3)
+        base = buf.ctypes.data  # the Array4 base: cell (lo_x, lo_y)
+        check(lib.ecg_upload_state(ctx.handle, base, -g, -g, js, ns), "upload", ctx.handle)
+        np.testing.assert_array_equal(ctx.download(), u0)
+        check(lib.ecg_euler_fv_one_step_host(ctx.handle, base, base, -g, -g, js, ns, dt, 0.0, None), "host step",
+              ctx.handle)
+        np.testing.assert_array_equal(box, pin_out)
+        box[...] = 0.0
+        check(lib.ecg_download_state(ctx.handle, base, -g, -g, js, ns), "download", ctx.handle)
+        np.testing.assert_array_equal(box, pin_out)
+        # the ghosts and the row and plane padding are untouched
+        inside = np.zeros(buf.size, dtype=bool)
+        np.lib.stride_tricks.as_strided(inside[g * js + g:], shape=u0.shape, strides=(ns, js, 1))[...] = True
+        assert np.isnan(buf[~inside]).all()
