@@ -86,6 +86,11 @@ struct GmresArgs {
   int prow;           // rows of a block (the last may have fewer)
   int det;            // grid sums in a fixed order (bit-reproducible solves)
   long long spin_limit;
+  // Chained solves (gmres_enqueue): gate[0] is set once a phase of the chain
+  // failed, gate[1] when a mixed solve left its system to the FP64 fallback.
+  // role 1: a chain's solve; role 2: its FP64 fallback.
+  int* gate;
+  int role;
 };
 
 // Grid-wide barrier over co-resident blocks (cooperative launch): one
@@ -1121,6 +1126,9 @@ template <bool RES, bool MIXED>
 __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
 {
   extern __shared__ double sh[];
+  // A gated solve whose chain already failed, or a fallback nobody needs,
+  // does nothing (every block reads the same flags, written before the launch).
+  if (a.gate && (__ldcg(a.gate) != 0 || (a.role == 2 && __ldcg(a.gate + 1) == 0))) return;
   unsigned int gen = 0;   // barriers passed; the counter is zeroed by the host before the launch
   unsigned int nred = 0;  // accumulator reductions completed
   unsigned int nset = 0;  // deterministic mode: partial-sum settles passed
@@ -1244,6 +1252,25 @@ __global__ void __launch_bounds__(NT) gmres_kernel(GmresArgs a)
     out.vec_access64 = S.cnt[0] + (final_known ? 0.0 : 4.0);  // the final residual: x, hx, hy, b
     out.vec_access32 = S.cnt[1];
     *a.res = out;
+    if (a.gate) {
+      // the caller's tests on the returned iterate's true residual, as the
+      // IMEX step takes them: a mixed solve ending finite above the rule is
+      // handed to the fallback, any other solve failing it stops the chain
+      const bool fin = isfinite(out.final_linf) && isfinite(out.final_b_linf);
+      if (a.role == 2) a.gate[1] = 0;
+      bool hand_over = false;
+      if (MIXED && a.role == 1 && !out.timeout && !out.nonfinite && fin) {
+        const double fb = out.final_b_linf < 1.0 ? 1.0 : out.final_b_linf;
+        hand_over = !(out.final_linf <= a.tol || out.final_linf / fb <= a.tol);
+      }
+      if (hand_over) {
+        a.gate[1] = 1;
+      } else {
+        const double bn = out.b_linf > 1.0 ? out.b_linf : 1.0;
+        const bool conv = fin && (out.final_linf <= a.tol || out.final_linf / bn <= a.tol);
+        if (out.timeout || !conv) a.gate[0] = 1;
+      }
+    }
   }
 }
 
@@ -1423,9 +1450,9 @@ void gmres_work_destroy(EcgGmresWork* w)
   delete w;
 }
 
-cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
-                        int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
-                        int reorth, bool det, EcgGmresResult* out, cudaStream_t s)
+cudaError_t gmres_enqueue(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
+                          int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
+                          int reorth, bool det, EcgGmresResult* d_res, int* gate, int role, cudaStream_t s)
 {
   if (mixed != w->mixed) return cudaErrorInvalidValue;  // the basis is allocated for one precision
   GmresArgs a;
@@ -1445,7 +1472,9 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   a.det = det ? 1 : 0;
   a.R = w->R;
   a.bar = w->bar;
-  a.res = w->d_res;
+  a.res = d_res ? d_res : w->d_res;
+  a.gate = gate;
+  a.role = gate ? role : 0;
   a.ld = w->ld;
   a.m = w->m;
   a.max_iter = max_iter < w->m ? max_iter : w->m;
@@ -1463,7 +1492,15 @@ cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* 
   e = cudaMemsetAsync(w->acc, 0, sizeof(double) * 3 * w->ld, s);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
-  e = cudaLaunchCooperativeKernel(gmres_entry(w->kres > 0, w->mixed), dim3(w->nblocks), dim3(NT), args, w->smem, s);
+  return cudaLaunchCooperativeKernel(gmres_entry(w->kres > 0, w->mixed), dim3(w->nblocks), dim3(NT), args, w->smem, s);
+}
+
+cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
+                        int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
+                        int reorth, bool det, EcgGmresResult* out, cudaStream_t s)
+{
+  cudaError_t e = gmres_enqueue(w, op, b, x0, x, max_iter, tol, mixed, inner_max_iter, inner_rtol, max_refine, reorth,
+                                det, nullptr, nullptr, 0, s);
   if (e != cudaSuccess) return e;
   e = cudaMemcpyAsync(w->h_res, w->d_res, sizeof(EcgGmresResult), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return e;

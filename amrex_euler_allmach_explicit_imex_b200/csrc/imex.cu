@@ -1,9 +1,16 @@
 // euler_imex_bdltv20_o1_source_map_picard_one_step on the device
 // (imex/imex_source_map_step.hpp:300-616): star update -> Picard iterations
 // {face enthalpies, pressure-row rhs, GMRES, gate, p <- x, eq54 momentum} ->
-// conservative closeout.  The state stays on the device; the host reads the
-// per-phase reductions (a few hundred bytes) to take the reference's
-// early-return decisions.
+// conservative closeout.  The state stays on the device.
+//
+// The whole step is queued at once and the host waits once, at its end.
+// Each phase writes its reductions to a slot of its own; the reference's
+// early-return tests run on the device (a one-thread gate kernel after the
+// star update, each assembly and each refresh; the GMRES kernel on its own
+// result), and once one fails every later phase is a no-op launch.  The host
+// then reads all slots and results (a few KB) and takes the reference's
+// decisions in the reference's order, so the diagnostics and the state are
+// those of the step that stopped where the first failing test stopped it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,12 +37,47 @@ struct EcgImexState {
   unsigned char* fyf = nullptr;
   double* rhs = nullptr;
   double* x = nullptr;
+  // reduction slots of one step: the star update, per Picard pass the
+  // assembly and the refresh, the matrix diagnostics, the closeout
+  int passes = -1;                   // Picard passes the slots were made for
   EcgImexStats* d_st = nullptr;
-  EcgImexStats* h_st = nullptr;  // pinned
-  EcgImexStats init{};           // reset template
+  EcgImexStats* h_st = nullptr;      // pinned
+  EcgImexStats* h_init = nullptr;    // pinned: the reset template in every slot
+  EcgGmresResult* d_res = nullptr;   // per pass: the solve, then its FP64 fallback
+  EcgGmresResult* h_res = nullptr;   // pinned
+  int* d_gate = nullptr;             // {a phase failed, a mixed solve needs the fallback}
   EcgGmresWork* gw = nullptr;
-  EcgGmresWork* gw64 = nullptr;  // mixed precision: FP64 workspace of the fallback solve, made on first use
+  EcgGmresWork* gw64 = nullptr;      // mixed precision: FP64 workspace of the fallback solve
 };
+
+namespace {
+constexpr int kSlotStar = 0;
+int slot_assemble(int k) { return 1 + 2 * k; }
+int slot_refresh(int k) { return 2 + 2 * k; }
+int slot_matrix(int passes) { return 1 + 2 * passes; }
+int slot_close(int passes) { return 2 + 2 * passes; }
+int slot_count(int passes) { return 3 + 2 * passes; }
+
+// The reference's early-return tests on a phase's reductions
+// (imex_source_map_step.hpp:405-454 after the star update, :464-497 after an
+// assembly, :536-564 after a refresh): gate[0] is set when the test fails.
+enum GateKind { kGateStar = 0, kGateAssemble = 1, kGateRefresh = 2 };
+
+__device__ bool key_is_finite(unsigned long long k)
+{
+  const unsigned long long b = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFULL) : ~k;
+  return isfinite(__longlong_as_double(static_cast<long long>(b)));
+}
+
+__global__ void imex_gate_kernel(const EcgImexStats* st, int kind, int* gate)
+{
+  bool fail;
+  if (kind == kGateStar) fail = st->floor_count > 0;
+  else if (kind == kGateAssemble) fail = st->row_nonfinite > 0 || !key_is_finite(st->rhs_linf_key);
+  else fail = st->k_nonfinite > 0;
+  if (fail) gate[0] = 1;
+}
+}  // namespace
 
 namespace {
 
@@ -108,9 +150,7 @@ bool ensure_state(ecg_ctx* c)
   alloc(reinterpret_cast<void**>(&im->fyf), nfy);
   alloc(reinterpret_cast<void**>(&im->rhs), sizeof(double) * n);
   alloc(reinterpret_cast<void**>(&im->x), sizeof(double) * n);
-  alloc(reinterpret_cast<void**>(&im->d_st), sizeof(EcgImexStats));
-  if (ok) ok = ecgi::cuda_ok(c, cudaMallocHost(&im->h_st, sizeof(EcgImexStats)), "imex host alloc");
-  im->init = stats_template();
+  alloc(reinterpret_cast<void**>(&im->d_gate), sizeof(int) * 2);
   if (ok) {
     std::string err;
     im->gw = gmres_work_create(n, max_iter < 1 ? 1 : max_iter, c->num_sms, c->device, mixed, &err);
@@ -118,22 +158,43 @@ bool ensure_state(ecg_ctx* c)
       c->err = err;
       ok = false;
     }
+    // the fallback solve is queued (gated) with every mixed solve, so its
+    // workspace exists from the start
+    if (ok && mixed) {
+      im->gw64 = gmres_work_create(n, max_iter < 1 ? 1 : max_iter, c->num_sms, c->device, false, &err);
+      if (!im->gw64) {
+        c->err = err;
+        ok = false;
+      }
+    }
   }
   return ok;
 }
 
-bool reset_stats(ecg_ctx* c)
+// Stats slots and result records for a step of `passes` Picard passes.
+bool ensure_slots(ecg_ctx* c, int passes)
 {
-  return ecgi::cuda_ok(c, cudaMemcpyAsync(c->imex->d_st, &c->imex->init, sizeof(EcgImexStats), cudaMemcpyHostToDevice,
-                                          c->stream), "reset stats");
-}
-
-bool fetch_stats(ecg_ctx* c)
-{
-  if (!ecgi::cuda_ok(c, cudaMemcpyAsync(c->imex->h_st, c->imex->d_st, sizeof(EcgImexStats), cudaMemcpyDeviceToHost,
-                                        c->stream), "fetch stats"))
-    return false;
-  return ecgi::cuda_ok(c, cudaStreamSynchronize(c->stream), "sync");
+  EcgImexState* im = c->imex;
+  if (im->passes >= passes) return true;
+  cudaFree(im->d_st);
+  cudaFreeHost(im->h_st);
+  cudaFreeHost(im->h_init);
+  cudaFree(im->d_res);
+  cudaFreeHost(im->h_res);
+  im->d_st = im->h_st = im->h_init = nullptr;
+  im->d_res = im->h_res = nullptr;
+  im->passes = -1;
+  const int ns = slot_count(passes), nr = 2 * (passes > 0 ? passes : 1);
+  const bool ok = ecgi::cuda_ok(c, cudaMalloc(&im->d_st, sizeof(EcgImexStats) * ns), "imex alloc") &&
+                  ecgi::cuda_ok(c, cudaMallocHost(&im->h_st, sizeof(EcgImexStats) * ns), "imex host alloc") &&
+                  ecgi::cuda_ok(c, cudaMallocHost(&im->h_init, sizeof(EcgImexStats) * ns), "imex host alloc") &&
+                  ecgi::cuda_ok(c, cudaMalloc(&im->d_res, sizeof(EcgGmresResult) * nr), "imex alloc") &&
+                  ecgi::cuda_ok(c, cudaMallocHost(&im->h_res, sizeof(EcgGmresResult) * nr), "imex host alloc");
+  if (!ok) return false;
+  const EcgImexStats t = stats_template();
+  for (int k = 0; k < ns; ++k) im->h_init[k] = t;
+  im->passes = passes;
+  return true;
 }
 
 double kd(unsigned long long k) { return ecgi::okey_to_double(k); }
@@ -185,6 +246,10 @@ void imex_free(ecg_ctx* c)
   if (im->gw64) gmres_work_destroy(im->gw64);
   cudaFree(im->d_st);
   cudaFreeHost(im->h_st);
+  cudaFreeHost(im->h_init);
+  cudaFree(im->d_res);
+  cudaFreeHost(im->h_res);
+  cudaFree(im->d_gate);
   gmres_work_destroy(im->gw);
   delete im;
   c->imex = nullptr;
@@ -200,34 +265,25 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     return ECG_ERR_UNSUPPORTED;
   }
   if (!ensure_state(c)) return ECG_ERR_CUDA;
+  const int passes = c->cfg.imex_picard_iterations > 0 ? c->cfg.imex_picard_iterations : 0;
+  if (!ensure_slots(c, passes)) return ECG_ERR_CUDA;
   EcgImexState* im = c->imex;
   const EcgImexOps* ops = c->opt.arith == ECG_ARITH_EXACT ? &ecg_imex_exact_ops : &ecg_imex_fast_ops;
   const bool mixed = c->opt.imex_precision == ECG_IMEX_MIXED;
+  const bool det = c->opt.deterministic != 0;
   ecg_imex_diag& d = *out;
   std::memset(&d, 0, sizeof(d));
   d.solver_status = ECG_SOLVER_NOT_RUN;
   d.linear_solver_status_last = -1;
   const double inf = std::numeric_limits<double>::infinity();
   const EcgFvParams P = ecgi::fv_params(c, true);
-  const EcgImexMap m = imex_map(c);
+  const EcgImexMap m = imex_map(c);  // ungated: the matrix diagnostics always run
+  EcgImexMap mg = m;                 // the phases that stop after a failed test
+  mg.abort = im->d_gate;
   const long long n = im->n;
   const double idx = c->grid.inv_dx, idy = c->grid.inv_dy;
+  const double tol = c->cfg.imex_solver_tol;
   cudaStream_t s = c->stream;
-
-  // star update and step initialisation (imex_source_map_step.hpp:405-454)
-  if (!reset_stats(c)) return ECG_ERR_CUDA;
-  if (!ecgi::cuda_ok(c, ops->star(P, c->cur_state(), dt, im->S, im->p, im->K, im->d_st, s), "star")) return ECG_ERR_CUDA;
-  if (!fetch_stats(c)) return ECG_ERR_CUDA;
-  EcgImexStats& st = *im->h_st;
-  d.kinetic_lag_nonfinite_count = static_cast<int>(st.k_nonfinite);
-  d.trial_density_min = kd(st.trial_rho_min_key);
-  d.density_denominator_floor_count = static_cast<int>(st.floor_count);
-  if (st.floor_count > 0) {
-    d.solver_status = ECG_SOLVER_DENSITY_DENOMINATOR_FLOOR_USED;
-    d.positivity_failure_count = static_cast<int>(st.floor_count);
-    return ECG_OK;
-  }
-  d.pressure_energy_residual_before_linf = st.mismatch_before_nonfinite ? inf : kd(st.mismatch_before_key);
 
   EcgPressureOp op;
   std::memset(&op, 0, sizeof(op));
@@ -241,70 +297,114 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
   op.yc = 0.25 * dt * dt * idy * idy;
   op.hx = im->hx;
   op.hy = im->hy;
-  const double tol = c->cfg.imex_solver_tol;
 
-  // Matrix diagnostics (imex_source_map_step.hpp:466-489) of the pressure
-  // system of the current Picard pass: reported for the pass that ends the
-  // step, so they are computed there, from that pass's face enthalpies.
-  auto matrix_report = [&]() -> bool {
-    if (!reset_stats(c)) return false;
-    if (!ecgi::cuda_ok(c, ops->matrix(m, im->hx, im->hy, dt, idx, idy, im->d_st, s), "matrix diagnostics")) return false;
-    if (!fetch_stats(c)) return false;
-    d.pressure_matrix_nonzeros = static_cast<int>(st.nnz);
-    d.pressure_matrix_max_row_width = static_cast<int>(st.max_row_width);
-    d.kinetic_jacobian_abs_max = kd(st.abs_max_key);
-    d.pressure_matrix_symmetry_linf = kd(st.sym_key);
-    return true;
+  // ---- queue the step ----------------------------------------------------------------
+  auto ok = [&](cudaError_t e, const char* what) { return ecgi::cuda_ok(c, e, what); };
+  auto gate = [&](int slot, int kind) {
+    imex_gate_kernel<<<1, 1, 0, s>>>(im->d_st + slot, kind, im->d_gate);
+    return ok(cudaGetLastError(), "gate");
   };
-
-  for (int pic = 0; pic < c->cfg.imex_picard_iterations; ++pic) {
+  if (!ok(cudaMemcpyAsync(im->d_st, im->h_init, sizeof(EcgImexStats) * slot_count(passes), cudaMemcpyHostToDevice, s),
+          "reset stats") ||
+      !ok(cudaMemsetAsync(im->d_gate, 0, sizeof(int) * 2, s), "reset gate"))
+    return ECG_ERR_CUDA;
+  // star update and step initialisation (imex_source_map_step.hpp:405-454)
+  if (!ok(ops->star(P, c->cur_state(), dt, im->S, im->p, im->K, im->d_st + kSlotStar, s), "star") ||
+      !gate(kSlotStar, kGateStar))
+    return ECG_ERR_CUDA;
+  for (int pic = 0; pic < passes; ++pic) {
     // pressure system (source_map_build_pressure_system, imex_source_map_step.hpp:8-38,464-497)
-    if (!reset_stats(c)) return ECG_ERR_CUDA;
-    if (!ecgi::cuda_ok(c, ops->assemble(m, im->S, im->p, im->K, im->hx, im->hy, dt, idx, idy, im->rhs, im->d_st, s),
-                       "assemble"))
+    if (!ok(ops->assemble(mg, im->S, im->p, im->K, im->hx, im->hy, dt, idx, idy, im->rhs, im->d_st + slot_assemble(pic),
+                          s),
+            "assemble") ||
+        !gate(slot_assemble(pic), kGateAssemble))
       return ECG_ERR_CUDA;
-    if (!fetch_stats(c)) return ECG_ERR_CUDA;
+    // The solve reports the true residuals before and after (||A p - b||inf,
+    // ||A x - b||inf and ||b||inf, pressure_residual's values) with its
+    // result.  A mixed solve that ends with a finite true residual above the
+    // rule (its iteration budget ran out, or its FP32 basis stalled) is
+    // finished by the FP64 solve from the iterate it reached, so the mixed
+    // step fails only where the FP64 step would.
+    if (!ok(gmres_enqueue(im->gw, op, im->rhs, im->p, im->x, c->cfg.imex_solver_max_iter, tol, mixed,
+                          c->opt.mixed_inner_max_iter, c->opt.mixed_inner_rtol, c->opt.mixed_max_refinements,
+                          c->opt.mixed_reorth, det, im->d_res + 2 * pic, im->d_gate, 1, s),
+            "gmres"))
+      return ECG_ERR_CUDA;
+    if (mixed && !ok(gmres_enqueue(im->gw64, op, im->rhs, im->x, im->x, c->cfg.imex_solver_max_iter, tol, false, 0,
+                                   0.0, 0, 1, det, im->d_res + 2 * pic + 1, im->d_gate, 2, s),
+                     "gmres fallback"))
+      return ECG_ERR_CUDA;
+    // p <- x, eq54 momentum refresh (imex_source_map_step.hpp:536-564), in one
+    // sweep: K from x, then x becomes the pressure buffer (no copy).  The
+    // buffers are renamed as queued: a step that stops early reaches no
+    // closeout, and the next step's star update rewrites p.
+    if (!ok(ops->refresh(mg, im->p, im->x, im->S, dt, idx, idy, im->K, im->d_st + slot_refresh(pic), s), "refresh") ||
+        !gate(slot_refresh(pic), kGateRefresh))
+      return ECG_ERR_CUDA;
+    std::swap(im->p, im->x);
+  }
+  // Matrix diagnostics (imex_source_map_step.hpp:466-489) of the pressure
+  // system of the last assembled pass: the pass that ended the step, whether
+  // it stopped early or not (the later passes' assemblies did nothing).
+  if (passes > 0 && !ok(ops->matrix(m, im->hx, im->hy, dt, idx, idy, im->d_st + slot_matrix(passes), s), "matrix"))
+    return ECG_ERR_CUDA;
+  // conservative closeout (evaluate_source_map_final, imex_source_map_step.hpp:75-258)
+  double* out_state = c->next_state();
+  if (!ok(ops->faces(mg, im->S, im->p, im->K, im->fx, im->fy, im->fxf, im->fyf, 1, s), "faces") ||
+      !ok(ops->closeout(mg, c->grid, im->S, im->p, im->K, im->fx, im->fy, im->fxf, im->fyf, dt, out_state,
+                        im->d_st + slot_close(passes), s),
+          "closeout") ||
+      !ok(ops->eq78(mg, c->grid, im->S, im->K, im->d_st + slot_close(passes), s), "eq78"))
+    return ECG_ERR_CUDA;
+  if (!ok(cudaMemcpyAsync(im->h_st, im->d_st, sizeof(EcgImexStats) * slot_count(passes), cudaMemcpyDeviceToHost, s),
+          "fetch stats") ||
+      (passes > 0 &&
+       !ok(cudaMemcpyAsync(im->h_res, im->d_res, sizeof(EcgGmresResult) * 2 * passes, cudaMemcpyDeviceToHost, s),
+           "fetch results")) ||
+      !ok(cudaStreamSynchronize(s), "sync"))
+    return ECG_ERR_CUDA;
+
+  // ---- the reference's decisions, in its order, on what the phases reported ----
+  const EcgImexStats* stp = &im->h_st[kSlotStar];
+  auto matrix_report = [&]() {
+    const EcgImexStats& ms = im->h_st[slot_matrix(passes)];
+    d.pressure_matrix_nonzeros = static_cast<int>(ms.nnz);
+    d.pressure_matrix_max_row_width = static_cast<int>(ms.max_row_width);
+    d.kinetic_jacobian_abs_max = kd(ms.abs_max_key);
+    d.pressure_matrix_symmetry_linf = kd(ms.sym_key);
+    return ECG_OK;
+  };
+  d.kinetic_lag_nonfinite_count = static_cast<int>(stp->k_nonfinite);
+  d.trial_density_min = kd(stp->trial_rho_min_key);
+  d.density_denominator_floor_count = static_cast<int>(stp->floor_count);
+  if (stp->floor_count > 0) {
+    d.solver_status = ECG_SOLVER_DENSITY_DENOMINATOR_FLOOR_USED;
+    d.positivity_failure_count = static_cast<int>(stp->floor_count);
+    return ECG_OK;
+  }
+  d.pressure_energy_residual_before_linf = stp->mismatch_before_nonfinite ? inf : kd(stp->mismatch_before_key);
+
+  for (int pic = 0; pic < passes; ++pic) {
+    const EcgImexStats& sa = im->h_st[slot_assemble(pic)];
     d.pressure_matrix_rows = static_cast<int>(n);
-    if (st.row_nonfinite > 0 || !std::isfinite(kd(st.rhs_linf_key))) {
+    if (sa.row_nonfinite > 0 || !std::isfinite(kd(sa.rhs_linf_key))) {
       d.solver_status = ECG_SOLVER_SOURCE_MAP_PRESSURE_ROW_NONFINITE;
-      d.kinetic_lag_nonfinite_count = static_cast<int>(st.row_nonfinite);
-      d.nonfinite_count = static_cast<int>(st.row_nonfinite);
-      return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
+      d.kinetic_lag_nonfinite_count = static_cast<int>(sa.row_nonfinite);
+      d.nonfinite_count = static_cast<int>(sa.row_nonfinite);
+      return matrix_report();
     }
-    // The solve reports the true residuals before and after
-    // (||A p - b||inf, ||A x - b||inf and ||b||inf, pressure_residual's values)
-    // with its result: no separate residual launches or host waits.
-    EcgGmresResult g;
-    if (!ecgi::cuda_ok(c, gmres_solve(im->gw, op, im->rhs, im->p, im->x, c->cfg.imex_solver_max_iter, tol, mixed,
-                                      c->opt.mixed_inner_max_iter, c->opt.mixed_inner_rtol,
-                                      c->opt.mixed_max_refinements, c->opt.mixed_reorth, c->opt.deterministic != 0, &g, s),
-                       "gmres"))
-      return ECG_ERR_CUDA;
+    EcgGmresResult g = im->h_res[2 * pic];
     if (g.timeout) {
       c->err = "gmres grid barrier timed out";
       return ECG_ERR_TIMEOUT;
     }
-    // A mixed solve that ends with a finite true residual above the rule
-    // (its iteration budget ran out, or its FP32 basis stalled) is finished
-    // by the FP64 solve from the iterate it reached, so the mixed step fails
-    // only where the FP64 step would.
     if (mixed && !g.nonfinite && std::isfinite(g.final_linf) && std::isfinite(g.final_b_linf) &&
         !(g.final_linf <= tol || g.final_linf / std::max(g.final_b_linf, 1.0) <= tol)) {
-      if (!im->gw64) {
-        std::string err;
-        im->gw64 = gmres_work_create(n, im->max_iter < 1 ? 1 : im->max_iter, c->num_sms, c->device, false, &err);
-        if (!im->gw64) {
-          c->err = err;
-          return ECG_ERR_CUDA;
-        }
-      }
+      // the FP64 fallback ran from the mixed iterate
       const double r0 = g.initial_linf, b0 = g.b_linf;
       const int its = g.iterations, inner = g.inner_iterations, cyc = g.refinements;
       const double bytes = static_cast<double>(n) * (8.0 * g.vec_access64 + 4.0 * g.vec_access32);
-      if (!ecgi::cuda_ok(c, gmres_solve(im->gw64, op, im->rhs, im->x, im->x, c->cfg.imex_solver_max_iter, tol, false, 0,
-                                        0.0, 0, 1, c->opt.deterministic != 0, &g, s),
-                         "gmres fallback"))
-        return ECG_ERR_CUDA;
+      g = im->h_res[2 * pic + 1];
       if (g.timeout) {
         c->err = "gmres grid barrier timed out";
         return ECG_ERR_TIMEOUT;
@@ -336,50 +436,32 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     const bool rel_ok = d.pressure_linear_residual_relative_linf <= tol;
     d.linear_solver_status_last = abs_ok ? ECG_SOLVER_CONVERGED_ABSOLUTE
                                          : (rel_ok ? ECG_SOLVER_CONVERGED_RELATIVE : ECG_SOLVER_LINEAR_SOLVE_NOT_CONVERGED);
-    if (!std::isfinite(lr) || nf || g.nonfinite) {
-      if (!std::isfinite(lr) || nf) {
-        d.solver_status = ECG_SOLVER_LINEAR_RESIDUAL_NONFINITE;
-        d.nonfinite_count = 1;
-        return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
-      }
+    if (!std::isfinite(lr) || nf) {
+      d.solver_status = ECG_SOLVER_LINEAR_RESIDUAL_NONFINITE;
+      d.nonfinite_count = 1;
+      return matrix_report();
     }
     if (!abs_ok && !rel_ok) {
       d.solver_status = g.breakdown ? ECG_SOLVER_GMRES_BREAKDOWN_NOT_CONVERGED : ECG_SOLVER_LINEAR_SOLVE_NOT_CONVERGED;
-      return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
+      return matrix_report();
     }
-    // p <- x, eq54 momentum refresh (imex_source_map_step.hpp:536-564), in one
-    // sweep: K from x, then x becomes the pressure buffer (no copy)
-    if (!reset_stats(c)) return ECG_ERR_CUDA;
-    if (!ecgi::cuda_ok(c, ops->refresh(m, im->p, im->x, im->S, dt, idx, idy, im->K, im->d_st, s), "refresh"))
-      return ECG_ERR_CUDA;
-    std::swap(im->p, im->x);
-    if (!fetch_stats(c)) return ECG_ERR_CUDA;
-    d.kinetic_lag_nonfinite_count = static_cast<int>(st.k_nonfinite);
-    if (st.k_nonfinite > 0) {
+    const EcgImexStats& sr = im->h_st[slot_refresh(pic)];
+    d.kinetic_lag_nonfinite_count = static_cast<int>(sr.k_nonfinite);
+    if (sr.k_nonfinite > 0) {
       d.solver_status = ECG_SOLVER_SOURCE_MAP_LAGGED_MOMENTUM_NONFINITE;
       d.nonfinite_count = d.kinetic_lag_nonfinite_count;
-      return matrix_report() ? ECG_OK : ECG_ERR_CUDA;
+      return matrix_report();
     }
     ++d.kinetic_lag_update_count;
-    d.pressure_picard_delta_linf = kd(st.delta_linf_key);
-    d.source_picard_delta_l2_relative_to_pmax = std::sqrt(st.delta_l2_sum / static_cast<double>(n)) / kd(st.pmax_key);
+    d.pressure_picard_delta_linf = kd(sr.delta_linf_key);
+    d.source_picard_delta_l2_relative_to_pmax = std::sqrt(sr.delta_l2_sum / static_cast<double>(n)) / kd(sr.pmax_key);
     ++d.source_picard_iterations_used;
     ++d.picard_pressure_solves_used;
   }
   d.solver_status = d.linear_solver_status_last;
-  if (c->cfg.imex_picard_iterations > 0 && !matrix_report()) return ECG_ERR_CUDA;
+  if (passes > 0) matrix_report();
 
-  // conservative closeout (evaluate_source_map_final, imex_source_map_step.hpp:75-258)
-  if (!reset_stats(c)) return ECG_ERR_CUDA;
-  if (!ecgi::cuda_ok(c, ops->faces(m, im->S, im->p, im->K, im->fx, im->fy, im->fxf, im->fyf, 1, s), "faces"))
-    return ECG_ERR_CUDA;
-  double* out_state = c->next_state();
-  if (!ecgi::cuda_ok(c, ops->closeout(m, c->grid, im->S, im->p, im->K, im->fx, im->fy, im->fxf, im->fyf, dt, out_state,
-                                      im->d_st, s),
-                     "closeout"))
-    return ECG_ERR_CUDA;
-  if (!ecgi::cuda_ok(c, ops->eq78(m, c->grid, im->S, im->K, im->d_st, s), "eq78")) return ECG_ERR_CUDA;
-  if (!fetch_stats(c)) return ECG_ERR_CUDA;
+  const EcgImexStats& st = im->h_st[slot_close(passes)];
   const int rcount = static_cast<int>(st.residual_count);
   const int nfc = static_cast<int>(st.final_nonfinite);
   double rl1 = 0.0, ml1 = 0.0, el1 = 0.0;

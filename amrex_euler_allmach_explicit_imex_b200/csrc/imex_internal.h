@@ -15,6 +15,9 @@ struct EcgImexMap {
   double gamma;
   double cst[4];    // bubble post-shock conserved state
   double p_fixed;   // bubble fixed post-shock pressure
+  // The step's phases are queued without host waits: once a phase has failed
+  // (*abort nonzero) the kernels given this map do nothing.  Null: always run.
+  const int* abort;
 };
 
 // Reductions of the IMEX kernels (min/max as ordered keys, counts, sums).
@@ -120,6 +123,18 @@ void gmres_work_destroy(EcgGmresWork* w);
 cudaError_t gmres_solve(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
                         int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
                         int reorth, bool det, EcgGmresResult* out, cudaStream_t s);
+// gmres_solve without waiting: the result lands in d_res (device memory).
+// gate (device int[2], may be null) chains the solve into a sequence of
+// launches the host does not wait between: gate[0] nonzero means an earlier
+// phase failed, gate[1] that a mixed solve left its system to the FP64
+// fallback.  role 1: skipped when gate[0] is set; sets gate[0] when the
+// returned iterate fails the acceptance rule (||A x - b||inf <= tol or
+// relative to max(||b||inf, 1)), or, for a mixed solve ending finite above
+// it, gate[1] instead.  role 2 (the FP64 fallback, from x): runs only when
+// gate[1] is set and gate[0] is not; clears gate[1], sets gate[0] on failure.
+cudaError_t gmres_enqueue(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x0, double* x,
+                          int max_iter, double tol, bool mixed, int inner_max_iter, double inner_rtol, int max_refine,
+                          int reorth, bool det, EcgGmresResult* d_res, int* gate, int role, cudaStream_t s);
 // r = A x - b: infinity norm, rhs infinity norm (max(|b|inf, 1)) and nonfinite flag.
 cudaError_t pressure_residual(EcgGmresWork* w, const EcgPressureOp& op, const double* b, const double* x,
                               double* res_linf, double* rhs_norm, int* nonfinite, cudaStream_t s);

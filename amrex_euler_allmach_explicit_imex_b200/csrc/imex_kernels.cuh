@@ -335,6 +335,10 @@ __global__ void __launch_bounds__(NT) imex_star_kernel(const EcgFvParams P, cons
 // every x-face (nx+1 per row) and y-face (ny+1 per column).  Thread c of row
 // j takes x-face (c, j) and y-face (c, j), which share the cell (c, j); rows
 // stride over grid.y, so no face index is divided.
+// A queued phase of a step whose earlier phase failed does nothing (the
+// flag was written before the launch, so every thread reads the same value).
+__device__ __forceinline__ bool gated_off(const EcgImexMap& m) { return m.abort && __ldcg(m.abort) != 0; }
+
 template <int NT>
 __global__ void __launch_bounds__(NT) imex_face_kernel(const EcgImexMap m, const double* __restrict__ S,
                                                        const double* __restrict__ p, const double* __restrict__ K,
@@ -342,6 +346,7 @@ __global__ void __launch_bounds__(NT) imex_face_kernel(const EcgImexMap m, const
                                                        unsigned char* __restrict__ fxf, unsigned char* __restrict__ fyf,
                                                        const int mode)
 {
+  if (gated_off(m)) return;
   const int c = blockIdx.x * NT + threadIdx.x;
   if (c > m.nx) return;
   for (int j = blockIdx.y; j <= m.ny; j += gridDim.y) {
@@ -495,6 +500,7 @@ __global__ void __launch_bounds__(NT) imex_assemble_kernel(const EcgImexMap m, c
                                                            double* __restrict__ rhs, EcgImexStats* __restrict__ st)
 {
   static_assert(NT == AX * AY, "one thread per cell of the tile");
+  if (gated_off(m)) return;
   __shared__ Shared sh;
   __shared__ double fx[AY][AX + 1];
   __shared__ double fy[AY + 1][AX];
@@ -729,6 +735,7 @@ __global__ void __launch_bounds__(NT) imex_refresh_kernel(const EcgImexMap m, co
                                                           const double dt, const double idx, const double idy,
                                                           double* __restrict__ K, EcgImexStats* __restrict__ st)
 {
+  if (gated_off(m)) return;
   __shared__ Shared sh;
   const long long n = static_cast<long long>(m.nx) * m.ny;
   unsigned long long dl = okey(0.0), pm = okey(1.0);
@@ -769,6 +776,7 @@ __global__ void __launch_bounds__(NT) imex_closeout_kernel(const EcgImexMap m, c
                                                            const unsigned char* __restrict__ fyf, const double dt,
                                                            double* __restrict__ out, EcgImexStats* __restrict__ st)
 {
+  if (gated_off(m)) return;
   __shared__ Shared sh;
   const long long n = static_cast<long long>(m.nx) * m.ny;
   const double gm1 = m.gamma - 1.0, idx = G.inv_dx, idy = G.inv_dy;
@@ -877,6 +885,7 @@ __global__ void __launch_bounds__(NT) imex_eq78_kernel(const EcgImexMap m, const
                                                        const double* __restrict__ S, const double* __restrict__ K,
                                                        EcgImexStats* __restrict__ st)
 {
+  if (gated_off(m)) return;
   __shared__ Shared sh;
   const long long n = static_cast<long long>(m.nx) * m.ny;
   const double idx = G.inv_dx, idy = G.inv_dy;

@@ -131,6 +131,55 @@ def test_imex_not_converged_and_floor_statuses(gpu, oracle):
         assert d.density_denominator_floor_count >= 1
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_imex_early_stop_reports_the_failing_pass(gpu, oracle, prec):
+    """The step's phases are queued without host waits and stop on the device
+    at the first failed test: a solve capped at 2 iterations fails in the
+    first Picard pass, so the later passes and the closeout do nothing, and
+    the diagnostics are those of the failing pass (its matrix, its residual,
+    no lag update), as the reference reports them.  In mixed precision the
+    FP64 fallback finishes the capped mixed solve from its iterate and fails
+    the same way."""
+    c = golden_io.imex_case("gresho_m0p01")
+    kv = dict(l.split("=", 1) for l in golden_io.kv_of(c["kv"]).split("\n"))
+    kv["euler.imex_solver_max_iter"] = 2
+    cfg = read_config(kv).cfg
+    ref_u1, ref_d = oracle.imex_step(cfg, c["u0"], float(c["dt"]))
+    with api.Context(cfg, imex_precision=prec) as ctx:
+        ctx.upload(c["u0"])
+        d = api.euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, float(c["dt"]))
+        assert np.array_equal(ctx.download(), c["u0"])
+        assert d.solver_status == ref_d.solver_status
+        for f in ["picard_pressure_solves_used", "source_picard_iterations_used", "kinetic_lag_update_count",
+                  "pressure_matrix_rows", "pressure_matrix_max_row_width", "nonfinite_count"]:
+            assert getattr(d, f) == getattr(ref_d, f), f
+        assert abs(d.pressure_matrix_nonzeros - ref_d.pressure_matrix_nonzeros) <= 0.01 * ref_d.pressure_matrix_nonzeros
+        assert d.kinetic_jacobian_abs_max == pytest.approx(ref_d.kinetic_jacobian_abs_max, rel=1e-9)
+        assert d.solver_initial_residual == pytest.approx(ref_d.solver_initial_residual, rel=1e-9)
+        # the capped solve stops at its limit (the fallback adds its own, at most 2)
+        if prec == "mixed":
+            assert ref_d.solver_iterations <= d.solver_iterations <= 4
+        else:
+            assert d.solver_iterations == ref_d.solver_iterations
+        assert d.gmres_fp64_fallbacks == (1 if prec == "mixed" else 0)
+        assert d.pressure_linear_residual_relative_linf > cfg.imex_solver_tol
+    # a step stopped at its first phase leaves the context ready: the next
+    # step from a good state runs to its end and matches the reference
+    kv["euler.imex_solver_max_iter"] = 200
+    cfg = read_config(kv).cfg
+    bad = c["u0"].copy()
+    bad[0, 3, 3] = 1e-16
+    bad[1:3, 3, 3] = 0.0
+    with api.Context(cfg, imex_precision=prec) as ctx:
+        ctx.upload(bad)
+        d = api.euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, float(c["dt"]))
+        assert api.solver_status_str(d.solver_status) == "density_denominator_floor_used"
+        ctx.upload(c["u0"])
+        d = api.euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, float(c["dt"]))
+        assert d.solver_status in (1, 2), api.solver_status_str(d.solver_status)
+        assert golden_io.state_rel_err(ctx.download(), c["u1"]) <= 1e-9
+
+
 def test_imex_device_loop_vs_oracle(gpu, oracle):
     """ecg_run for the IMEX method: 3 steps of the Gresho M=0.1 case."""
     c = golden_io.imex_case("gresho_m0p1")
