@@ -76,6 +76,7 @@ class GpuOptions(C.Structure):
         ("mixed_reorth", C.c_int32),
         ("stream", C.c_void_p),
         ("deterministic", C.c_int32),
+        ("mixed_min_iterations", C.c_int32),
     ]
 
 
@@ -164,7 +165,7 @@ IMEX_DIAG_REAL_FIELDS = [
 
 
 # fields after the reals, not in the reference
-IMEX_DIAG_TAIL_FIELDS = ["gmres_fp64_fallbacks", "pad_end"]
+IMEX_DIAG_TAIL_FIELDS = ["gmres_fp64_fallbacks", "gmres_fp32_basis"]
 
 
 class ImexDiag(C.Structure):

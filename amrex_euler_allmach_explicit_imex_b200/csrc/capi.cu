@@ -348,6 +348,7 @@ void ecg_default_gpu_options(ecg_gpu_options* o)
   o->mixed_inner_rtol = 1.0e-3;
   o->mixed_max_refinements = 12;
   o->mixed_reorth = 0;
+  o->mixed_min_iterations = 8;
   o->tile_x = 0;
   o->tile_y = 0;
   o->stream = nullptr;

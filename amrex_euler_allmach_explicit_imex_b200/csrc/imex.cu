@@ -47,7 +47,8 @@ struct EcgImexState {
   EcgGmresResult* h_res = nullptr;   // pinned
   int* d_gate = nullptr;             // {a phase failed, a mixed solve needs the fallback}
   EcgGmresWork* gw = nullptr;
-  EcgGmresWork* gw64 = nullptr;      // mixed precision: FP64 workspace of the fallback solve
+  EcgGmresWork* gw64 = nullptr;      // mixed precision: FP64 workspace of the fallback (and of short) solves
+  double last_its = -1.0;            // iterations per solve of the previous step (-1: none yet)
 };
 
 namespace {
@@ -269,12 +270,20 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
   if (!ensure_slots(c, passes)) return ECG_ERR_CUDA;
   EcgImexState* im = c->imex;
   const EcgImexOps* ops = c->opt.arith == ECG_ARITH_EXACT ? &ecg_imex_exact_ops : &ecg_imex_fast_ops;
-  const bool mixed = c->opt.imex_precision == ECG_IMEX_MIXED;
+  // Mixed precision puts a step's solves on the FP32 basis unless the
+  // previous step's solves were short (mixed_min_iterations): their basis
+  // stays in L2, and the restart cycle the FP32 basis needs to reach the
+  // tolerance costs more iterations than the halved bytes save.
+  const bool mixed = c->opt.imex_precision == ECG_IMEX_MIXED &&
+                     !(c->opt.mixed_min_iterations > 0 && im->last_its >= 0.0 &&
+                       im->last_its < static_cast<double>(c->opt.mixed_min_iterations));
+  EcgGmresWork* const gw = mixed || !im->gw64 ? im->gw : im->gw64;
   const bool det = c->opt.deterministic != 0;
   ecg_imex_diag& d = *out;
   std::memset(&d, 0, sizeof(d));
   d.solver_status = ECG_SOLVER_NOT_RUN;
   d.linear_solver_status_last = -1;
+  d.gmres_fp32_basis = mixed ? 1 : 0;
   const double inf = std::numeric_limits<double>::infinity();
   const EcgFvParams P = ecgi::fv_params(c, true);
   const EcgImexMap m = imex_map(c);  // ungated: the matrix diagnostics always run
@@ -325,7 +334,7 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     // rule (its iteration budget ran out, or its FP32 basis stalled) is
     // finished by the FP64 solve from the iterate it reached, so the mixed
     // step fails only where the FP64 step would.
-    if (!ok(gmres_enqueue(im->gw, op, im->rhs, im->p, im->x, c->cfg.imex_solver_max_iter, tol, mixed,
+    if (!ok(gmres_enqueue(gw, op, im->rhs, im->p, im->x, c->cfg.imex_solver_max_iter, tol, mixed,
                           c->opt.mixed_inner_max_iter, c->opt.mixed_inner_rtol, c->opt.mixed_max_refinements,
                           c->opt.mixed_reorth, det, im->d_res + 2 * pic, im->d_gate, 1, s),
             "gmres"))
@@ -365,6 +374,16 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
     return ECG_ERR_CUDA;
 
   // ---- the reference's decisions, in its order, on what the phases reported ----
+  // (the iterations per solve of the passes that ran pick the next step's basis)
+  struct SolveCount {
+    EcgImexState* im;
+    int solves = 0;
+    double its = 0.0;
+    ~SolveCount()
+    {
+      if (solves > 0) im->last_its = its / solves;
+    }
+  } count{im};
   const EcgImexStats* stp = &im->h_st[kSlotStar];
   auto matrix_report = [&]() {
     const EcgImexStats& ms = im->h_st[slot_matrix(passes)];
@@ -394,6 +413,8 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
       return matrix_report();
     }
     EcgGmresResult g = im->h_res[2 * pic];
+    count.solves += 1;
+    count.its += g.inner_iterations;
     if (g.timeout) {
       c->err = "gmres grid barrier timed out";
       return ECG_ERR_TIMEOUT;
@@ -405,6 +426,7 @@ extern "C" ecg_status ecg_imex_step(ecg_ctx* c, double dt, ecg_imex_diag* out)
       const int its = g.iterations, inner = g.inner_iterations, cyc = g.refinements;
       const double bytes = static_cast<double>(n) * (8.0 * g.vec_access64 + 4.0 * g.vec_access32);
       g = im->h_res[2 * pic + 1];
+      count.its += g.inner_iterations;
       if (g.timeout) {
         c->err = "gmres grid barrier timed out";
         return ECG_ERR_TIMEOUT;

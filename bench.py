@@ -350,7 +350,7 @@ def imex_leg(dev, stream, steps=3, only_case=None):
                              stream=stream.cuda_stream) as ctx:
                 api.initialize_state(ctx)
                 t = 0.0
-                ms, its, statuses, gbytes = [], [], [], []
+                ms, its, statuses, gbytes, fp32 = [], [], [], [], []
                 for k in range(steps + 1):
                     dt, _ = api.compute_imex_dt(ctx, t)
                     a = torch.cuda.Event(enable_timing=True)
@@ -364,6 +364,7 @@ def imex_leg(dev, stream, steps=3, only_case=None):
                         ms.append(a.elapsed_time(b))
                         its.append(d.gmres_inner_iterations if prec == "mixed" else d.solver_iterations)
                         gbytes.append(d.gmres_vector_bytes)
+                        fp32.append(d.gmres_fp32_basis)
                     t += dt
                 states[prec] = ctx.download()
                 if prec == "fp64_again":
@@ -373,6 +374,7 @@ def imex_leg(dev, stream, steps=3, only_case=None):
                 other = cells * (IMEX_STAR_B + cfg.imex_picard_iterations * IMEX_PICARD_B + IMEX_CLOSE_B)
                 step_bytes = gb + other
                 out[prec] = {"ms_per_step": med, "gmres_iterations": its, "status": statuses[-1],
+                             "fp32_basis_steps": sum(fp32),
                              "step_statuses": statuses, "gmres_bytes_per_step": gb, "step_bytes": step_bytes,
                              "achieved_gbs": step_bytes / (med * 1e-3) / 1e9,
                              "hbm_frac": step_bytes / (med * 1e-3) / 1e9 / peak}

@@ -162,6 +162,10 @@ typedef struct ecg_gpu_options {
   int32_t deterministic;    /* 1: the GMRES grid sums run in a fixed block order, so repeated IMEX steps on
                                the same inputs give the same bits (a little slower); 0 (default): atomic
                                accumulation, whose order can change the last bits from run to run */
+  int32_t mixed_min_iterations; /* mixed: a step whose previous step's pressure solves took fewer iterations
+                                   than this on average solves on the FP64 basis (short solves stay in L2,
+                                   where the FP32 basis saves nothing and its restart cycle costs
+                                   iterations); 0: always the FP32 basis.  Default 8. */
 } ecg_gpu_options;
 
 /* Diagnostics (core/basic_diagnostics.hpp:3-7). */
@@ -269,7 +273,8 @@ typedef struct ecg_imex_diag {
   int32_t gmres_fp64_fallbacks;       /* mixed precision: Picard solves the FP32-basis cycles left above the
                                          tolerance and the FP64 solve finished from their iterate (not in the
                                          reference) */
-  int32_t pad_end;
+  int32_t gmres_fp32_basis;           /* mixed precision: 1 when the step's solves ran on the FP32 basis, 0 when
+                                         mixed_min_iterations sent them to the FP64 solve (not in the reference) */
 } ecg_imex_diag;
 
 /* Result of a device-resident time loop (driver_main.hpp:224-333). */

@@ -249,3 +249,37 @@ def test_imex_mach122_variant_against_oracle(gpu, oracle, prec):
     assert ref_d.solver_status in (1, 2)
     assert d.solver_status in (1, 2), api.solver_status_str(d.solver_status)
     assert golden_io.state_rel_err(u1, ref_u1) <= 1e-9
+
+
+def test_mixed_short_solves_take_the_fp64_basis(gpu):
+    """mixed_min_iterations: once a step's solves average fewer iterations
+    than the bound (the shock-density bubble's take 4-5), the next step
+    solves on the FP64 basis; bound 0 keeps the FP32 basis on every step.
+    Both converge every step and stay within the GMRES rounding of the FP64
+    run."""
+    kv = {"amr.n_cell": "160 40", "geometry.prob_hi": "2 0.5", "euler.problem": "shock_density_bubble_2d",
+          "euler.method": "imex", "euler.spatial_order": 2, "euler.imex_cfl": 0.45,
+          "euler.imex_picard_iterations": 4, "euler.imex_solver_tol": 1e-10, "euler.imex_solver_max_iter": 200,
+          "euler.imex_acoustic_startup": 0, "euler.imex_acoustic_cfl_cap": 0}
+    cfg = read_config(kv).cfg
+
+    def run(**gpu_kw):
+        with api.Context(cfg, **gpu_kw) as ctx:
+            api.initialize_state(ctx)
+            t, basis = 0.0, []
+            for _ in range(3):
+                dt, _ = api.compute_imex_dt(ctx, t)
+                d = api.euler_imex_bdltv20_o1_source_map_picard_one_step(ctx, dt)
+                assert d.solver_status in (1, 2), api.solver_status_str(d.solver_status)
+                basis.append(d.gmres_fp32_basis)
+                t += dt
+            return ctx.download(), basis
+
+    ref, b64 = run()
+    assert b64 == [0, 0, 0]
+    u, b = run(imex_precision="mixed")
+    assert b == [1, 0, 0]
+    assert golden_io.state_rel_err(u, ref) <= 1e-9
+    u, b = run(imex_precision="mixed", mixed_min_iterations=0)
+    assert b == [1, 1, 1]
+    assert golden_io.state_rel_err(u, ref) <= 1e-9
