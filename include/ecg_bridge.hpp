@@ -40,6 +40,9 @@
  *   ecg.imex_precision = fp64 (default) | mixed (FP32-stored Krylov basis)
  *   ecg.device         = CUDA device ordinal (default 0)
  *   ecg.deterministic  = 0 (default) | 1 (GMRES sums in a fixed order)
+ *   ecg.mixed_min_iterations = 8 (default): with mixed, a step after solves
+ *                        that averaged fewer iterations solves on the FP64
+ *                        basis; 0 keeps the FP32 basis on every step
  *
  * Errors from the library end the run through amrex::Abort with its message.
  */
@@ -140,6 +143,7 @@ inline ecg_gpu_options gpu_options()
   int v = 0;
   if (pp.query("device", v)) o.device = v;
   if (pp.query("deterministic", v)) o.deterministic = v;
+  if (pp.query("mixed_min_iterations", v)) o.mixed_min_iterations = v;
   return o;
 }
 
