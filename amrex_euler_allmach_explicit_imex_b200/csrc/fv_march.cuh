@@ -47,9 +47,10 @@ __device__ __forceinline__ Prim minus_half(const Prim& q, const Prim& s)
 // path (independent instruction streams the scheduler can interleave); faces
 // that need the reference path (degenerate HLLC star state, sound speed off
 // the rsqrt path) are recomputed after one warp vote.  deg_*: HLLC fell back
-// to Rusanov on that face.
+// to Rusanov on that face.  Returns whether the vote fired (the same on every
+// lane): deg_* can only be set then.
 template <int RK>
-__device__ __forceinline__ void face_pair(Prim xl, Prim xr, Prim yl, Prim yr, double g, double inv_gm1, Cons& fx,
+__device__ __forceinline__ bool face_pair(Prim xl, Prim xr, Prim yl, Prim yr, double g, double inv_gm1, Cons& fx,
                                           Cons& fy, bool& deg_x, bool& deg_y)
 {
   if (RK == ECG_RIEMANN_LOWMACH_HLLC) {
@@ -73,7 +74,9 @@ __device__ __forceinline__ void face_pair(Prim xl, Prim xr, Prim yl, Prim yr, do
       if (bx) fx = fast::hllc_f(xl, xr, 0, g, inv_gm1, deg_x);
       if (by) fy = fast::hllc_f(yl, yr, 1, g, inv_gm1, deg_y);
     }
+    return true;
   }
+  return false;
 }
 
 // One face with the warp-voting flux (faces evaluated one after the other).
@@ -161,16 +164,16 @@ __device__ __forceinline__ void march_strip(const EcgFvParams& P, const double* 
     // evaluates both (lanes 0, 1 and 31 cost nothing extra in lockstep), only
     // lanes 2..30 use or count their x-face
     Cons fl, gt;
-    bool deg_x, deg_y;
+    bool deg_x, deg_y, voted = true;
     if (PAIR) {
-      face_pair<RK>(plus_half(ql, sxl), minus_half(qc, sx), plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), g,
-                    inv_gm1, fl, gt, deg_x, deg_y);
+      voted = face_pair<RK>(plus_half(ql, sxl), minus_half(qc, sx), plus_half(qc, sy_cur), minus_half(L.q[2], sy_next),
+                            g, inv_gm1, fl, gt, deg_x, deg_y);
     } else {
       gt = face_w<RK>(plus_half(qc, sy_cur), minus_half(L.q[2], sy_next), 1, g, inv_gm1, deg_y);
       fl = face_w<RK>(plus_half(ql, sxl), minus_half(qc, sx), 0, g, inv_gm1, deg_x);
     }
     const Cons fr{shdn(fl.rho), shdn(fl.mx), shdn(fl.my), shdn(fl.E)};
-    if (count_deg) {
+    if (count_deg && voted) {
       // each face counts once per adjacent cell of this strip in the domain
       // (count_hllc_degenerate_star_states, explicit_update.hpp:2-56)
       const bool left_ok = lane >= 3 && lane <= 2 + kCells && x - 1 < nx;
@@ -259,11 +262,18 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
   double* const col = &ring.v[0][0][lane];
   const unsigned col_s = static_cast<unsigned>(__cvta_generic_to_shared(col));
   unsigned flips = 0;  // bit (row mod kRing): that staged row is a mirror image (my to negate)
+  // Strips whose 32 columns all lie in the domain take in-domain rows
+  // straight from the state, at a pointer that moves one row a request (the
+  // rows are requested in order); the ghost policy decides the rest.
+  const bool xin = c0 >= 2 && c0 + kLanes - 2 <= nx;
+  const long long pitch = P.g.pitch, pl = P.g.plane;
+  const double* rowp = u + static_cast<long long>(j0 - 2) * pitch + x;  // dereferenced only when in the domain
   // request row jr of this lane's column (an empty group past the strip's rows)
   auto put = [&](int jr) {
     if (jr <= jlast) {
       const int sl = jr & (kRing - 1);
-      const CellSrc c = cell_src(P, u, x, jr);
+      const CellSrc c = xin && static_cast<unsigned>(jr) < static_cast<unsigned>(ny) ? CellSrc{rowp, pl, false}
+                                                                                     : cell_src(P, u, x, jr);
       flips = c.flip ? (flips | (1u << sl)) : (flips & ~(1u << sl));
       if (c.p) {
         const unsigned d = col_s + static_cast<unsigned>(sl * 4 * kLanes * 8);
@@ -279,6 +289,7 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
         d[3 * kLanes] = P.bc.cst[3];
       }
     }
+    rowp += pitch;
     cp_async_commit();
   };
   auto get = [&](int jr) {
@@ -307,8 +318,8 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
     g0 = face_one<RK>(plus_half(q_m1, sy_m1), minus_half(qa, s0), 1, g, inv_gm1, deg);
     if (count_deg && deg && cell_ok && j0 < ny) acc.degenerate += 1;
   }
-  const long long pl = P.g.plane;
   double* const obase = out + xs;
+  double rate_max = kLowest, rho_min = kMax, p_min = kMax;
 
   // one row: row j's cells from rows j (q0), j+1 (q1) and the new row j+2
   // (into q2), the y-slope of row j (sc; that of row j+1 into sn) and the
@@ -323,18 +334,19 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
     const Prim sx = slope3<LIM>(ql, q0, qr, second);
     const Prim sxl{shup(sx.rho), shup(sx.u), shup(sx.v), shup(sx.p)};
     Cons fl;
-    bool deg_x, deg_y;
+    bool deg_x, deg_y, voted = true;
     if (PAIR) {
-      face_pair<RK>(plus_half(ql, sxl), minus_half(q0, sx), plus_half(q0, sc), minus_half(q1, sn), g, inv_gm1, fl,
-                    gt, deg_x, deg_y);
+      voted = face_pair<RK>(plus_half(ql, sxl), minus_half(q0, sx), plus_half(q0, sc), minus_half(q1, sn), g, inv_gm1,
+                            fl, gt, deg_x, deg_y);
     } else {
       gt = face_w<RK>(plus_half(q0, sc), minus_half(q1, sn), 1, g, inv_gm1, deg_y);
       fl = face_w<RK>(plus_half(ql, sxl), minus_half(q0, sx), 0, g, inv_gm1, deg_x);
     }
     const Cons fr{shdn(fl.rho), shdn(fl.mx), shdn(fl.my), shdn(fl.E)};
-    if (count_deg) {
+    if (count_deg && voted) {
       // each face counts once per adjacent cell of this strip in the domain
-      // (count_hllc_degenerate_star_states, explicit_update.hpp:2-56)
+      // (count_hllc_degenerate_star_states, explicit_update.hpp:2-56); a
+      // face is degenerate only where the warp's fallback vote fired
       const bool left_ok = lane >= 3 && lane <= 2 + kCells && x - 1 < nx;
       if (deg_x && xface) acc.degenerate += (left_ok ? 1 : 0) + (cell_ok ? 1 : 0);
       if (deg_y && cell_ok) acc.degenerate += 1 + (j + 1 < jend ? 1 : 0);
@@ -354,11 +366,13 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
       o[pl] = n.mx;
       o[2 * pl] = n.my;
       o[3 * pl] = n.E;
+      // running extrema as doubles (max/min skip a NaN operand, as the keys'
+      // NaN test does), turned into ordered keys once, after the strip
       const double rate = (fabs(q.u) + cs) * idx + (fabs(q.v) + cs) * idy;
-      if (!isnan(rate)) acc.kmax = umax64(acc.kmax, okey(rate));
+      rate_max = fmax(rate_max, rate);
       const bool bad = !isfinite(q.rho) || !isfinite(q.u) || !isfinite(q.v) || !isfinite(q.p) || !isfinite(n.E);
-      acc.krho = umin64(acc.krho, okey(bad ? -kInf : q.rho));
-      acc.kp = umin64(acc.kp, okey(bad ? -kInf : q.p));
+      rho_min = fmin(rho_min, bad ? -kInf : q.rho);
+      p_min = fmin(p_min, bad ? -kInf : q.p);
       acc.nonfinite += bad ? 1 : 0;
     }
   };
@@ -374,6 +388,9 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
     g0 = g1;
   }
   cp_async_wait<0>();  // no request outlives the strip
+  acc.kmax = umax64(acc.kmax, okey(rate_max));
+  acc.krho = umin64(acc.krho, okey(rho_min));
+  acc.kp = umin64(acc.kp, okey(p_min));
 }
 
 // Registers: the register-loaded strips at most 128 a thread (4 blocks of 4
