@@ -342,6 +342,78 @@ static __device__ __noinline__ Cons xie_f(const Prim l, const Prim r, int axis, 
   return out;
 }
 
+// xie_f without branches: the flux of a face whose states take none of
+// xie_f's exits (sound speeds on the rsqrt path, ordered wave speeds, and for
+// a subsonic face no degenerate denominator, square roots on their fast path
+// and a finite result), evaluated with xie_f's arithmetic in xie_f's order;
+// a supersonic face selects the upwind physical flux as xie_f returns it.
+// `fallback` marks the faces xie_f must evaluate instead (the caller does so
+// after one warp vote); deg: the HLLC degeneracy test, valid without fallback.
+__device__ __forceinline__ Cons xie_core(const Prim& l, const Prim& r, int axis, double g, double inv_gm1,
+                                         double sensor, bool& fallback, bool& deg)
+{
+  const double ql = normal_vel(l, axis), qr = normal_vel(r, axis);
+  const double pl = l.p, pr = r.p;
+  bool bl, br;
+  const double cl = fsound_core(l.rho, pl, g, bl), cr = fsound_core(r.rho, pr, g, br);
+  const double sl = smin(ql - cl, qr - cr), sr = smax(ql + cl, qr + cr);
+  const bool ordered = sl < sr;
+  const bool sup_l = sl >= 0.0, sup_r = sr <= 0.0;
+  const bool supersonic = sup_l || sup_r;
+  const double al = l.rho * (sl - ql), ar = r.rho * (sr - qr);
+  const double ad = ar - al;
+  const double inv_ad = frcp(ad);
+  const double sm = (r.p - l.p + al * ql - ar * qr) * -inv_ad;
+  deg = !supersonic && (fabs(sl - sm) <= 1.0e-12 || fabs(sr - sm) <= 1.0e-12);
+  const double ss = (ar * qr - al * ql + pl - pr) * inv_ad;
+  const double dl = sl - ss, dr = sr - ss;
+  const Cons ul = to_cons_f(l, inv_gm1), ur = to_cons_f(r, inv_gm1);
+  const double ps = (ar * pl - al * pr - al * ar * (ql - qr)) * inv_ad;
+  const double srl = l.rho * frsqrt(l.rho), srr = r.rho * frsqrt(r.rho);
+  const double rd = srl + srr;
+  const double ird = frcp(rd);
+  const double uh = (srl * l.u + srr * r.u) * ird;
+  const double vh = (srl * l.v + srr * r.v) * ird;
+  const double qh = axis == 0 ? uh : vh;
+  const double hl = fdiv(ul.E + pl, l.rho), hr = fdiv(ur.E + pr, r.rho);
+  const double hh = (srl * hl + srr * hr) * ird;
+  const double c2 = (g - 1.0) * (hh - 0.5 * (uh * uh + vh * vh));
+  const double ch = c2 * frsqrt(c2);
+  const double mh = fdiv(qh, smax(ch, 1.0e-12));
+  // |u| of a state at rest is fsqrt's sqrt(0) = 0: kept on the fast path
+  const double sp2l = l.u * l.u + l.v * l.v, sp2r = r.u * r.u + r.v * r.v;
+  const bool okl = pos_normal_range(sp2l), okr = pos_normal_range(sp2r);
+  const double spl = okl ? sp2l * frsqrt(sp2l) : sp2l, spr = okr ? sp2r * frsqrt(sp2r) : sp2r;
+  const double th = clamp01(smax(fdiv(spl, smax(cl, 1.0e-12)), fdiv(spr, smax(cr, 1.0e-12))));
+  const double f = clamp01(sensor);
+  const double pss = th * ps + (1.0 - th) * 0.5 * (pl + pr);
+  const double psss = f * pss + (1.0 - f) * ps;
+  const double bp = fdiv((f - 1.0) * sl * sr * (pr - pl), (sr - sl) * (c2 * (1.0 + fabs(mh))));
+  const double nxv = axis == 0 ? 1.0 : 0.0, nyv = axis == 1 ? 1.0 : 0.0;
+  const bool left = ss >= 0.0;
+  const Prim q = left ? l : r;
+  const double qn = left ? ql : qr;
+  const double a = left ? al : ar;
+  const double rs = fdiv(a, left ? dl : dr);
+  const double e = left ? fdiv(ul.E, l.rho) : fdiv(ur.E, r.rho);
+  const double es = e + (ss - qn) * (ss + fdiv(left ? pl : pr, a));
+  const double rss = rs * ss;
+  const Cons sub{rss + bp, rss * (q.u + nxv * (ss - qn)) + nxv * psss + bp * uh,
+                 rss * (q.v + nyv * (ss - qn)) + nyv * psss + bp * vh,
+                 ss * (rs * es + ps) + 0.5 * bp * (uh * uh + vh * vh)};
+  // xie_f's exits of a subsonic face, and the square roots fsqrt would take
+  // off its rsqrt path (l.rho, r.rho, c2, the speeds; 0 < x < 1e300 there)
+  const bool sub_exit = fabs(ad) <= 1.0e-12 || fabs(dl) <= 1.0e-12 || fabs(dr) <= 1.0e-12 ||
+                        fabs(al) <= 1.0e-12 || fabs(ar) <= 1.0e-12 || !pos_normal_range(l.rho) ||
+                        !pos_normal_range(r.rho) || !(rd > 0.0) || !(c2 > 0.0) || !isfinite(c2) ||
+                        !pos_normal_range(c2) || !(okl || sp2l == 0.0) || !(okr || sp2r == 0.0) ||
+                        !isfinite(sub.rho) || !isfinite(sub.mx) || !isfinite(sub.my) || !isfinite(sub.E);
+  fallback = bl || br || !ordered || (!supersonic && sub_exit);
+  if (!supersonic) return sub;
+  const Prim& w = sup_l ? l : r;
+  return pflux(w, sup_l ? ul : ur, axis);
+}
+
 // Face pressure ratio of the multiface sensor (reconstruction_fluxes.hpp:390-397):
 // min(pl/pr, pr/pl) of the floored face pressures = min/max.
 __device__ __forceinline__ double pratio_f(double pl_in, double pr_in)
@@ -441,7 +513,69 @@ fv_fast_kernel(const EcgFvParams P, const double* __restrict__ u, double* __rest
   // ---- one x-face and one y-face per thread (threads tid < NF) ----
   int degenerate = 0;
   Cons fxv{0.0, 0.0, 0.0, 0.0}, fyv{0.0, 0.0, 0.0, 0.0};
-  if (tid < NF) {
+  if constexpr (XIE) {
+    // Every thread evaluates the branch-free core of a face (threads past the
+    // tile's faces repeat face 0 and discard it), so each warp can send the
+    // faces that take one of xie_f's exits through xie_f after one vote.
+    const int tf = tid < NF ? tid : 0;
+    const double* sy = sl + 4 * S::SN;
+    {
+      const int fx = tf % (T + 1), y = tf / (T + 1);
+      const int wl = (fx >= 1 && i0 + fx - 1 < nx) ? 1 : 0;
+      const int wr = (fx < T && i0 + fx < nx) ? 1 : 0;
+      const bool valid = tid < NF && j0 + y < ny && (wl | wr);
+      const int cl = R(fx - 1, y), cr = R(fx, y), sL = SI(fx - 1, y), sR = SI(fx, y);
+      const Prim L{fma(0.5, sl[sL], q_r[cl]), fma(0.5, sl[S::SN + sL], q_u[cl]), fma(0.5, sl[2 * S::SN + sL], q_v[cl]),
+                   fma(0.5, sl[3 * S::SN + sL], q_p[cl])};
+      const Prim Rr{fma(-0.5, sl[sR], q_r[cr]), fma(-0.5, sl[S::SN + sR], q_u[cr]),
+                    fma(-0.5, sl[2 * S::SN + sR], q_v[cr]), fma(-0.5, sl[3 * S::SN + sR], q_p[cr])};
+      double m = xr[(y + 1) * (T + 1) + fx];
+      m = smin(m, yr[y * (T + 2) + fx]);
+      m = smin(m, yr[(y + 1) * (T + 2) + fx]);
+      m = smin(m, yr[y * (T + 2) + fx + 1]);
+      m = smin(m, yr[(y + 1) * (T + 2) + fx + 1]);
+      const double h = clamp01(m);
+      bool fb, deg;
+      Cons f = xie_core(L, Rr, 0, g, inv_gm1, h * h * h, fb, deg);
+      fb = fb && valid;
+      if (__any_sync(0xffffffffu, fb)) {
+        if (fb) f = xie_f(L, Rr, 0, g, inv_gm1, h * h * h, deg);
+      }
+      if (valid) {
+        fxv = f;
+        if (ctl.count_degenerate && deg) degenerate += wl + wr;
+      }
+    }
+    {
+      const int x = tf % T, fy = tf / T;
+      const int wb = (fy >= 1 && j0 + fy - 1 < ny) ? 1 : 0;
+      const int wt = (fy < T && j0 + fy < ny) ? 1 : 0;
+      const bool valid = tid < NF && i0 + x < nx && (wb | wt);
+      const int cb = R(x, fy - 1), ct = R(x, fy), sB = SI(x, fy - 1), sT = SI(x, fy);
+      const Prim L{fma(0.5, sy[sB], q_r[cb]), fma(0.5, sy[S::SN + sB], q_u[cb]), fma(0.5, sy[2 * S::SN + sB], q_v[cb]),
+                   fma(0.5, sy[3 * S::SN + sB], q_p[cb])};
+      const Prim Rr{fma(-0.5, sy[sT], q_r[ct]), fma(-0.5, sy[S::SN + sT], q_u[ct]),
+                    fma(-0.5, sy[2 * S::SN + sT], q_v[ct]), fma(-0.5, sy[3 * S::SN + sT], q_p[ct])};
+      // x-face ratios at (x, fy-1), (x+1, fy-1), (x, fy), (x+1, fy)
+      double m = yr[fy * (T + 2) + x + 1];
+      m = smin(m, xr[fy * (T + 1) + x]);
+      m = smin(m, xr[fy * (T + 1) + x + 1]);
+      m = smin(m, xr[(fy + 1) * (T + 1) + x]);
+      m = smin(m, xr[(fy + 1) * (T + 1) + x + 1]);
+      const double h = clamp01(m);
+      bool fb, deg;
+      Cons f = xie_core(L, Rr, 1, g, inv_gm1, h * h * h, fb, deg);
+      fb = fb && valid;
+      if (__any_sync(0xffffffffu, fb)) {
+        if (fb) f = xie_f(L, Rr, 1, g, inv_gm1, h * h * h, deg);
+      }
+      if (valid) {
+        fyv = f;
+        if (ctl.count_degenerate && deg) degenerate += wb + wt;
+      }
+    }
+  }
+  if (!XIE && tid < NF) {
     // x-face fx between cells fx-1 and fx, row y
     const int fx = tid % (T + 1), y = tid / (T + 1);
     const int wl = (fx >= 1 && i0 + fx - 1 < nx) ? 1 : 0;
@@ -470,7 +604,7 @@ fv_fast_kernel(const EcgFvParams P, const double* __restrict__ u, double* __rest
       if (ctl.count_degenerate && deg) degenerate += wl + wr;
     }
   }
-  if (tid < NF) {
+  if (!XIE && tid < NF) {
     // y-face fy between cells (x, fy-1) and (x, fy)
     const int x = tid % T, fy = tid / T;
     const int wb = (fy >= 1 && j0 + fy - 1 < ny) ? 1 : 0;
