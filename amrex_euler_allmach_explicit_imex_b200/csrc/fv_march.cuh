@@ -240,6 +240,37 @@ __device__ __forceinline__ void cp_async_wait()
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// The multiface sensor's pressure ratio (xie_pressure_ratio_from_states,
+// reconstruction_fluxes.hpp:390-397) of the x-face on this lane's left in a
+// row of which this lane holds the pressure pc: the face pressures of the
+// MUSCL states, as the tile kernel forms them.
+template <int LIM>
+__device__ __forceinline__ double xface_ratio(double pc, bool second)
+{
+  const double pl = shup(pc), pr = shdn(pc);
+  const double s = second ? limited_slope(pc - pl, pr - pc, LIM) : 0.0;
+  return fast::pratio_f(fma(0.5, shup(s), pl), fma(-0.5, s, pc));
+}
+
+// xie_am_hllc_p flux of one face with sensor h^3 (reconstruction_fluxes.hpp:
+// 254-371, 390-440): the branch-free core, repaired by xie_f on the faces a
+// warp vote sends back.  deg: the HLLC degeneracy test of the face.
+__device__ __forceinline__ Cons face_xie(const Prim& l, const Prim& r, int axis, double g, double inv_gm1, double h,
+                                         bool& deg)
+{
+  const double sensor = h * h * h;
+  bool fb;
+  Cons f = fast::xie_core(l, r, axis, g, inv_gm1, sensor, fb, deg);
+  if (__any_sync(0xffffffffu, fb)) {
+    if (fb) f = fast::xie_f(l, r, axis, g, inv_gm1, sensor, deg);
+  }
+  return f;
+}
+
+// RK = xie_am_hllc_p: the faces one at a time, each with its 5-face sensor.
+// The pressure ratios it needs come along the march: the y-faces' below and
+// above row j (carried, and this row's), and the x-faces' of rows j and j+1
+// (row j+1's from the pressure of the window's next row, carried on).
 template <int RK, int LIM, bool PAIR>
 __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const double* __restrict__ u,
                                                    double* __restrict__ out, int c0, int j0, int H, double dt,
@@ -307,6 +338,8 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
   Prim qa, qb, qc;  // rows j, j+1 and the slot of row j+2, by role
   Prim s0, s1;      // y-slope of row j, and the slot of row j+1's
   Cons g0, g1;      // y-face below row j, and the slot of the face above it
+  constexpr bool XIE = RK == ECG_RIEMANN_XIE_AM_HLLC_P;
+  double yr_prev = 0.0, xr_cur = 0.0;  // XIE: pressure ratios of the y-face below row j, the x-face left of row j
   {
     const Prim q_m2 = fast::to_prim_f(get(j0 - 2), g);
     const Prim q_m1 = fast::to_prim_f(get(j0 - 1), g);
@@ -315,7 +348,20 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
     const Prim sy_m1 = slope3<LIM>(q_m2, q_m1, qa, second);
     s0 = slope3<LIM>(q_m1, qa, qb, second);
     bool deg;
-    g0 = face_one<RK>(plus_half(q_m1, sy_m1), minus_half(qa, s0), 1, g, inv_gm1, deg);
+    if constexpr (XIE) {
+      const Prim yl = plus_half(q_m1, sy_m1), yr = minus_half(qa, s0);
+      yr_prev = fast::pratio_f(yl.p, yr.p);
+      const double xm1 = xface_ratio<LIM>(q_m1.p, second);
+      xr_cur = xface_ratio<LIM>(qa.p, second);
+      double m = yr_prev;
+      m = smin(m, xm1);
+      m = smin(m, shdn(xm1));
+      m = smin(m, xr_cur);
+      m = smin(m, shdn(xr_cur));
+      g0 = face_xie(yl, yr, 1, g, inv_gm1, clamp01(m), deg);
+    } else {
+      g0 = face_one<RK>(plus_half(q_m1, sy_m1), minus_half(qa, s0), 1, g, inv_gm1, deg);
+    }
     if (count_deg && deg && cell_ok && j0 < ny) acc.degenerate += 1;
   }
   double* const obase = out + xs;
@@ -335,7 +381,29 @@ __device__ __forceinline__ void march_strip_staged(const EcgFvParams& P, const d
     const Prim sxl{shup(sx.rho), shup(sx.u), shup(sx.v), shup(sx.p)};
     Cons fl;
     bool deg_x, deg_y, voted = true;
-    if (PAIR) {
+    if constexpr (XIE) {
+      // sensors: the x-face on the left, from its own ratio and the y-faces'
+      // below and above cells i-1 and i; the y-face above, from its own ratio
+      // and the x-faces' left and right of cell i in rows j and j+1
+      const Prim xl = plus_half(ql, sxl), xrs = minus_half(q0, sx);
+      const Prim yl = plus_half(q0, sc), yrs = minus_half(q1, sn);
+      const double yr_cur = fast::pratio_f(yl.p, yrs.p);
+      const double xr_next = xface_ratio<LIM>(q1.p, second);
+      double my = yr_cur;
+      my = smin(my, xr_cur);
+      my = smin(my, shdn(xr_cur));
+      my = smin(my, xr_next);
+      my = smin(my, shdn(xr_next));
+      double mx = xr_cur;
+      mx = smin(mx, shup(yr_prev));
+      mx = smin(mx, shup(yr_cur));
+      mx = smin(mx, yr_prev);
+      mx = smin(mx, yr_cur);
+      gt = face_xie(yl, yrs, 1, g, inv_gm1, clamp01(my), deg_y);
+      fl = face_xie(xl, xrs, 0, g, inv_gm1, clamp01(mx), deg_x);
+      yr_prev = yr_cur;
+      xr_cur = xr_next;
+    } else if (PAIR) {
       voted = face_pair<RK>(plus_half(ql, sxl), minus_half(q0, sx), plus_half(q0, sc), minus_half(q1, sn), g, inv_gm1,
                             fl, gt, deg_x, deg_y);
     } else {
@@ -416,7 +484,7 @@ fv_march_kernel(const EcgFvParams P, const double* __restrict__ u, double* __res
   MarchAcc acc;
   acc.init();
   if (c0 < P.g.nx) {
-    if (STAGE)
+    if constexpr (STAGE)
       march_strip_staged<RK, LIM, PAIR>(P, u, out, c0, j0, H, dt, ctl.count_degenerate != 0, acc,
                                         ring[STAGE ? threadIdx.x >> 5 : 0]);
     else
@@ -488,7 +556,20 @@ inline cudaError_t launch(const EcgFvParams& p, const double* in, double* out, E
   switch (p.riemann) {
     case ECG_RIEMANN_RUSANOV: return launch_mode<ECG_RIEMANN_RUSANOV>(p, in, out, stats, ctl, s, pair, stage);
     case ECG_RIEMANN_LOWMACH_HLLC: return launch_mode<ECG_RIEMANN_LOWMACH_HLLC>(p, in, out, stats, ctl, s, pair, stage);
-    case ECG_RIEMANN_XIE_AM_HLLC_P: return fast::launch(p, in, out, stats, ctl, s);  // needs the 5-face sensor
+    case ECG_RIEMANN_XIE_AM_HLLC_P: {
+      // Staged strips carry the 5-face sensor along, on grids whose strips
+      // fill a wave of resident warps with runs of 8 rows or more (2560x640:
+      // 139 us against the tile kernel's 176 us); smaller grids, and the
+      // other variants, use the 16x16 tile kernel (Gresho 256^2: 19 us
+      // against 34 us on strips).
+      const long long strips = (p.g.nx + kCells - 1) / kCells;
+      const int rlo = p.row_hi > 0 ? p.row_lo : 0;
+      const int rhi = p.row_hi > 0 && p.row_hi < p.g.ny ? p.row_hi : p.g.ny;
+      const long long slots = static_cast<long long>(p.sm_count > 0 ? p.sm_count : 148) * 12;
+      if (stage && strips * ((rhi - rlo + 7) / 8) >= slots)
+        return launch_rk<ECG_RIEMANN_XIE_AM_HLLC_P, false, true>(p, in, out, stats, ctl, s);
+      return fast::launch(p, in, out, stats, ctl, s);
+    }
     default: return launch_mode<ECG_RIEMANN_HLLC>(p, in, out, stats, ctl, s, pair, stage);
   }
 }

@@ -150,6 +150,31 @@ def test_full_size_properties(gpu, riemann):
         assert abs(s1 - s0) <= 1e-12 * np.abs(u0[k]).sum()
 
 
+def test_hllcp_strips_match_the_tile_kernel(gpu):
+    """xie_am_hllc_p on the 2560x640 bubble: the staged strips (default; the
+    5-face sensor carried along the march) against the 16x16 tile kernel
+    (tile_y 1) over three steps: the same face formulas, so the states agree
+    to rounding and the degenerate counts and time steps are equal."""
+    kv = {"euler.problem": "shock_density_bubble_2d", "amr.n_cell": "2560 640", "geometry.prob_hi": "2 0.5",
+          "euler.riemann": "xie_am_hllc_p"}
+    cfg = read_config(kv).cfg
+    runs = {}
+    for tile in (0, 1):
+        with api.Context(cfg, tile_y=tile) as ctx:
+            api.initialize_state(ctx)
+            t, rec = 0.0, []
+            for _ in range(3):
+                dt = api.compute_euler_dt(ctx, t)
+                deg = api.euler_fv_one_step(ctx, dt, t)
+                rec.append((dt, deg))
+                t += dt
+            runs[tile] = (ctx.download(), rec)
+    assert golden_io.state_rel_err(runs[0][0], runs[1][0]) <= 3e-13
+    for (dt0, deg0), (dt1, deg1) in zip(runs[0][1], runs[1][1]):
+        assert dt0 == pytest.approx(dt1, rel=1e-13)
+        assert deg0 == deg1
+
+
 def test_full_size_bubble_matches_oracle_on_a_band(gpu, oracle):
     """The 2560x640 bubble step against the oracle on the full grid."""
     kv = {"euler.problem": "shock_density_bubble_2d", "amr.n_cell": "2560 640"}
