@@ -1,6 +1,7 @@
 // IMEX stencil kernels built with -fmad=true (default arithmetic mode).
 #include <string>
 #define ECG_NS ecg_fast
+#define ECG_IMEX_FAST_DIV 1
 #include "imex_kernels.cuh"
 
 const EcgImexOps ecg_imex_fast_ops = {ecg_fast::imex_star,     ecg_fast::imex_faces, ecg_fast::imex_matrix,

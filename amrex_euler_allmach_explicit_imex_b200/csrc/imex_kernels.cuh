@@ -29,6 +29,34 @@ constexpr double kInf = __builtin_huge_val();
 constexpr double kLowest = -1.7976931348623157e308;
 constexpr double kMax = 1.7976931348623157e308;
 
+// Division in the state-update arithmetic: IEEE in the exact build; in the
+// fast build (ECG_IMEX_FAST_DIV) the hardware reciprocal refined by one
+// third-order step y (1 + e + e^2), e = 1 - b y (a few units in the last
+// place), for divisors of magnitude in (1e-300, 1e300); IEEE otherwise.
+__device__ __forceinline__ double qdiv(double a, double b)
+{
+#ifdef ECG_IMEX_FAST_DIV
+  const double ab = fabs(b);
+  if (ab < 1.0e300 && ab > 1.0e-300) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    const double e = fma(-b, y, 1.0);
+    return a * fma(y, fma(e, e, e), y);
+  }
+#endif
+  return a / b;
+}
+
+// to_primitive (core/state_primitives.hpp:103-111) with qdiv
+__device__ __forceinline__ Prim to_prim_q(const Cons& c, double g)
+{
+  const double inv_rho = qdiv(1.0, c.rho);
+  const double u = c.mx * inv_rho;
+  const double v = c.my * inv_rho;
+  const double kin = 0.5 * c.rho * (u * u + v * v);
+  return Prim{c.rho, u, v, (g - 1.0) * (c.E - kin)};
+}
+
 __device__ __forceinline__ int wrapi(int i, int n)
 {
   int r = i % n;
@@ -131,25 +159,18 @@ struct FaceOut {
   int flags;  // bit0 guard, bit1 enthalpy inputs nonfinite, bit2 flux nonfinite
 };
 
-// source_map_face_flux_detail (imex_source_map_helpers.hpp:359-402)
-__device__ __forceinline__ FaceOut face_detail(const EcgImexMap& m, const double* __restrict__ S,
-                                               const double* __restrict__ p, const double* __restrict__ K, int il,
-                                               int jl, int ir, int jr, int axis)
+// source_map_face_flux_detail (imex_source_map_helpers.hpp:359-402) from the
+// face's two boundary-mapped densities, pressures and normal lagged momenta
+__device__ __forceinline__ FaceOut face_math(double gamma, double rho_l, double rho_r, double pl, double pr,
+                                             double ql, double qr)
 {
-  const double gm1 = m.gamma - 1.0;
-  const Cons L = state_b(m, S, il, jl), R = state_b(m, S, ir, jr);
-  double ml0, ml1, mr0, mr1;
-  m_b(m, K, il, jl, ml0, ml1);
-  m_b(m, K, ir, jr, mr0, mr1);
-  const double pl = p_b(m, p, il, jl), pr = p_b(m, p, ir, jr);
-  const double hl = m.gamma * pl / (gm1 * L.rho);
-  const double hr = m.gamma * pr / (gm1 * R.rho);
-  const double ql = axis == 0 ? ml0 : ml1;
-  const double qr = axis == 0 ? mr0 : mr1;
+  const double gm1 = gamma - 1.0;
+  const double hl = qdiv(gamma * pl, gm1 * rho_l);
+  const double hr = qdiv(gamma * pr, gm1 * rho_r);
   const double den = ql + qr;
   const double scale = smax(smax(fabs(ql), fabs(qr)), 1.0);
   const int guard = fabs(den) <= 1.0e-14 * scale ? 1 : 0;
-  const double h = guard ? 0.5 * (hl + hr) : (hl * ql + hr * qr) / den;
+  const double h = guard ? 0.5 * (hl + hr) : qdiv(hl * ql + hr * qr, den);
   const double mh = 0.5 * (ql + qr);
   FaceOut o;
   o.h_hat = h;
@@ -157,6 +178,19 @@ __device__ __forceinline__ FaceOut face_detail(const EcgImexMap& m, const double
   o.flags = guard | ((!isfinite(hl) || !isfinite(hr) || !isfinite(h) || !isfinite(ql) || !isfinite(qr)) ? 2 : 0) |
             (isfinite(o.flux) ? 0 : 4);
   return o;
+}
+
+// source_map_face_flux_detail of the face between cells (il, jl) and (ir, jr)
+__device__ __forceinline__ FaceOut face_detail(const EcgImexMap& m, const double* __restrict__ S,
+                                               const double* __restrict__ p, const double* __restrict__ K, int il,
+                                               int jl, int ir, int jr, int axis)
+{
+  const Cons L = state_b(m, S, il, jl), R = state_b(m, S, ir, jr);
+  double ml0, ml1, mr0, mr1;
+  m_b(m, K, il, jl, ml0, ml1);
+  m_b(m, K, ir, jr, mr0, mr1);
+  const double pl = p_b(m, p, il, jl), pr = p_b(m, p, ir, jr);
+  return face_math(m.gamma, L.rho, R.rho, pl, pr, axis == 0 ? ml0 : ml1, axis == 0 ? mr0 : mr1);
 }
 
 // ---- block reduction helpers ------------------------------------------------------
@@ -248,7 +282,7 @@ __device__ __forceinline__ Prim recon_cmm(const Cons& um, const Cons& u, const C
 {
   const Cons s{minmod(u.rho - um.rho, up.rho - u.rho), minmod(u.mx - um.mx, up.mx - u.mx),
                minmod(u.my - um.my, up.my - u.my), minmod(u.E - um.E, up.E - u.E)};
-  return to_prim(Cons{u.rho + h * s.rho, u.mx + h * s.mx, u.my + h * s.my, u.E + h * s.E}, g);
+  return to_prim_q(Cons{u.rho + h * s.rho, u.mx + h * s.mx, u.my + h * s.my, u.E + h * s.E}, g);
 }
 
 // bdltv20_pressure_split_lf_flux with material speed, reconstruction_fluxes.hpp:462-484,504-515
@@ -278,46 +312,83 @@ __device__ __forceinline__ Cons old_cell(const EcgFvParams& P, const double* __r
 // the step's initialisation fused in: p0 = pressure of U^n
 // (imex_source_map_step.hpp:422-434), K0 = star momentum (:418), the density
 // floor check (:436-451) and the star pressure mismatch (:278-298,453-454).
+constexpr int SX = 32, SY = 8;              // cells of a star tile
+constexpr int SHX = SX + 4, SHY = SY + 4;   // staged old state: columns c0-2 .. c0+SX+1, rows j0-2 .. j0+SY+1
 template <int NT>
 __global__ void __launch_bounds__(NT) imex_star_kernel(const EcgFvParams P, const double* __restrict__ u,
                                                        const double dt, double* __restrict__ S, double* __restrict__ p,
                                                        double* __restrict__ K, EcgImexStats* __restrict__ st)
 {
+  static_assert(NT == SX * SY, "one thread per cell of the tile");
   __shared__ Shared sh;
+  // A block takes a tile of SX x SY cells: the old state of the tile and a
+  // two-cell ring (the IMEX ghost policy applied once per cell), then each
+  // x- and y-face flux of the tile once (the per-cell form evaluates every
+  // face twice), then the update of its cells.
+  __shared__ double us[4][SHY][SHX];
+  __shared__ double fxs[4][SY][SX + 1];
+  __shared__ double fys[4][SY + 1][SX];
   const int nx = P.g.nx, ny = P.g.ny;
   const long long n = static_cast<long long>(nx) * ny;
   const double g = P.gamma, idx = P.g.inv_dx, idy = P.g.inv_dy;
+  const int c0 = blockIdx.x * SX, j0 = blockIdx.y * SY;
+  for (int e = threadIdx.x; e < SHX * SHY; e += NT) {
+    const int ex = e % SHX, ey = e / SHX;
+    const Cons c = old_cell(P, u, c0 - 2 + ex, j0 - 2 + ey);
+    us[0][ey][ex] = c.rho;
+    us[1][ey][ex] = c.mx;
+    us[2][ey][ex] = c.my;
+    us[3][ey][ex] = c.E;
+  }
+  __syncthreads();
+  auto cell = [&](int ex, int ey) { return Cons{us[0][ey][ex], us[1][ey][ex], us[2][ey][ex], us[3][ey][ex]}; };
+  // x-face f of row y lies between staged cells (f + 1, y + 2) and (f + 2, y + 2)
+  for (int e = threadIdx.x; e < SY * (SX + 1); e += NT) {
+    const int f = e % (SX + 1), y = e / (SX + 1);
+    const int ey = y + 2;
+    const Cons a = cell(f, ey), b = cell(f + 1, ey), c = cell(f + 2, ey), d = cell(f + 3, ey);
+    const Cons fl = split_lf(recon_cmm(a, b, c, 0.5, g), recon_cmm(b, c, d, -0.5, g), 0, g);
+    fxs[0][y][f] = fl.rho;
+    fxs[1][y][f] = fl.mx;
+    fxs[2][y][f] = fl.my;
+    fxs[3][y][f] = fl.E;
+  }
+  // y-face f of column x lies between staged cells (x + 2, f + 1) and (x + 2, f + 2)
+  for (int e = threadIdx.x; e < (SY + 1) * SX; e += NT) {
+    const int x = e % SX, f = e / SX;
+    const int ex = x + 2;
+    const Cons a = cell(ex, f), b = cell(ex, f + 1), c = cell(ex, f + 2), d = cell(ex, f + 3);
+    const Cons fl = split_lf(recon_cmm(a, b, c, 0.5, g), recon_cmm(b, c, d, -0.5, g), 1, g);
+    fys[0][f][x] = fl.rho;
+    fys[1][f][x] = fl.mx;
+    fys[2][f][x] = fl.my;
+    fys[3][f][x] = fl.E;
+  }
+  __syncthreads();
   long long floor_count = 0, knf = 0;
   unsigned long long rho_min = okey(kInf), mis = okey(0.0);
   long long mis_nf = 0;
-  for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
-       r += static_cast<long long>(gridDim.x) * NT) {
-    const int j = static_cast<int>(static_cast<unsigned>(r) / static_cast<unsigned>(nx)), i = static_cast<int>(r) - j * nx;
-    const Cons c = old_cell(P, u, i, j);
-    const Cons w = old_cell(P, u, i - 1, j), e = old_cell(P, u, i + 1, j);
-    const Cons s_ = old_cell(P, u, i, j - 1), nn = old_cell(P, u, i, j + 1);
-    const Cons ww = old_cell(P, u, i - 2, j), ee = old_cell(P, u, i + 2, j);
-    const Cons ss = old_cell(P, u, i, j - 2), n2 = old_cell(P, u, i, j + 2);
-    const Cons fxl = split_lf(recon_cmm(ww, w, c, 0.5, g), recon_cmm(w, c, e, -0.5, g), 0, g);
-    const Cons fxr = split_lf(recon_cmm(w, c, e, 0.5, g), recon_cmm(c, e, ee, -0.5, g), 0, g);
-    const Cons fyb = split_lf(recon_cmm(ss, s_, c, 0.5, g), recon_cmm(s_, c, nn, -0.5, g), 1, g);
-    const Cons fyt = split_lf(recon_cmm(s_, c, nn, 0.5, g), recon_cmm(c, nn, n2, -0.5, g), 1, g);
-    const Cons up{c.rho - dt * ((fxr.rho - fxl.rho) * idx + (fyt.rho - fyb.rho) * idy),
-                  c.mx - dt * ((fxr.mx - fxl.mx) * idx + (fyt.mx - fyb.mx) * idy),
-                  c.my - dt * ((fxr.my - fxl.my) * idx + (fyt.my - fyb.my) * idy),
-                  c.E - dt * ((fxr.E - fxl.E) * idx + (fyt.E - fyb.E) * idy)};
+  const int tx = threadIdx.x % SX, ty = threadIdx.x / SX;
+  const int i = c0 + tx, j = j0 + ty;
+  if (i < nx && j < ny) {
+    const long long r = static_cast<long long>(j) * nx + i;
+    const Cons c = cell(tx + 2, ty + 2);
+    const Cons up{c.rho - dt * ((fxs[0][ty][tx + 1] - fxs[0][ty][tx]) * idx + (fys[0][ty + 1][tx] - fys[0][ty][tx]) * idy),
+                  c.mx - dt * ((fxs[1][ty][tx + 1] - fxs[1][ty][tx]) * idx + (fys[1][ty + 1][tx] - fys[1][ty][tx]) * idy),
+                  c.my - dt * ((fxs[2][ty][tx + 1] - fxs[2][ty][tx]) * idx + (fys[2][ty + 1][tx] - fys[2][ty][tx]) * idy),
+                  c.E - dt * ((fxs[3][ty][tx + 1] - fxs[3][ty][tx]) * idx + (fys[3][ty + 1][tx] - fys[3][ty][tx]) * idy)};
     S[r] = up.rho;
     S[r + n] = up.mx;
     S[r + 2 * n] = up.my;
     S[r + 3 * n] = up.E;
     K[r] = up.mx;
     K[r + n] = up.my;
-    const double p0 = to_prim(c, g).p;
+    const double p0 = to_prim_q(c, g).p;
     p[r] = p0;
     if (!isfinite(up.mx) || !isfinite(up.my)) ++knf;
     if (!isfinite(up.rho) || up.rho <= 1.0e-14) ++floor_count;
     if (isfinite(up.rho)) rho_min = umin64(rho_min, okey(up.rho));
-    const double kin = 0.5 * (up.mx * up.mx + up.my * up.my) / up.rho;
+    const double kin = qdiv(0.5 * (up.mx * up.mx + up.my * up.my), up.rho);
     const double pe = (g - 1.0) * (up.E - kin);
     if (!isfinite(pe) || !isfinite(p0)) ++mis_nf;
     else mis = umax64(mis, okey(fabs(p0 - pe)));
@@ -421,13 +492,20 @@ __device__ __forceinline__ void row_terms(const EcgImexMap& m, const double* __r
   }
 }
 
+// The cell values a pressure row reads (boundary-mapped as
+// source_map_state_at_physical_boundary and the lagged-momentum lookup map
+// them): its star state and lagged momentum, the x-momentum of its east and
+// west neighbours and the y-momentum of its north and south neighbours.
+struct RowData {
+  double rho, mx, my, E, k0, k1, mx_e, mx_w, my_n, my_s;
+};
+
 // Right-hand side of row (i, j) of source_map_pressure_row_data
 // (imex_source_map_helpers.hpp:488-570) from the row's four face enthalpies;
 // rnf counts its nonfinite terms.
-__device__ __forceinline__ double rhs_row(const EcgImexMap& m, const double* __restrict__ S,
-                                          const double* __restrict__ K, double he, double hw, double hn, double hs,
-                                          int i, int j, double dt, double idx, double idy, double xc, double yc,
-                                          int& rnf)
+__device__ __forceinline__ double rhs_math(const EcgImexMap& m, const RowData& d, double he, double hw, double hn,
+                                           double hs, int i, double dt, double idx, double idy, double xc, double yc,
+                                           int& rnf)
 {
   const double gm1 = m.gamma - 1.0;
   rnf = 0;
@@ -448,33 +526,30 @@ __device__ __forceinline__ double rhs_row(const EcgImexMap& m, const double* __r
       }
     }
   }
-  const Cons s = star_at(m, S, i, j);
-  double k0, k1;
-  m_at(m, K, i, j, k0, k1);
-  const double kin = 0.5 * (k0 * k0 + k1 * k1) / s.rho;
+  const double kin = qdiv(0.5 * (d.k0 * d.k0 + d.k1 * d.k1), d.rho);
   double v;
-  v = s.E;
+  v = d.E;
   if (!isfinite(v)) ++rnf;
   b += v;
   v = -kin;
   if (!isfinite(v)) ++rnf;
   b += v;
-  v = -0.5 * dt * idx * he * state_b(m, S, i + 1, j).mx;
+  v = -0.5 * dt * idx * he * d.mx_e;
   if (!isfinite(v)) ++rnf;
   b += v;
-  v = -0.5 * dt * idx * (he - hw) * s.mx;
+  v = -0.5 * dt * idx * (he - hw) * d.mx;
   if (!isfinite(v)) ++rnf;
   b += v;
-  v = 0.5 * dt * idx * hw * state_b(m, S, i - 1, j).mx;
+  v = 0.5 * dt * idx * hw * d.mx_w;
   if (!isfinite(v)) ++rnf;
   b += v;
-  v = -0.5 * dt * idy * hn * state_b(m, S, i, j + 1).my;
+  v = -0.5 * dt * idy * hn * d.my_n;
   if (!isfinite(v)) ++rnf;
   b += v;
-  v = -0.5 * dt * idy * (hn - hs) * s.my;
+  v = -0.5 * dt * idy * (hn - hs) * d.my;
   if (!isfinite(v)) ++rnf;
   b += v;
-  v = 0.5 * dt * idy * hs * state_b(m, S, i, j - 1).my;
+  v = 0.5 * dt * idy * hs * d.my_s;
   if (!isfinite(v)) ++rnf;
   b += v;
   if (!isfinite(b)) ++rnf;
@@ -484,14 +559,18 @@ __device__ __forceinline__ double rhs_row(const EcgImexMap& m, const double* __r
 // The assembly of one Picard pass in one kernel: the eq46 face enthalpies
 // (imex_face_kernel, mode 0) and the right-hand side of
 // source_map_pressure_row_data (imex_source_map_helpers.hpp:488-570) with its
-// nonfinite count.  A block takes a tile of AX columns x AY rows of cells:
-// every thread evaluates the x-face on its cell's left and the y-face below
-// it, the tile's right x-faces and top y-faces are evaluated once more by 40
-// threads (they belong to the neighbour tiles, which store them), and the
-// rows' right-hand sides read all four faces from shared memory instead of
-// from global memory.  Tiles run over the face columns 0 .. nx and rows
-// 0 .. ny.
+// nonfinite count.  A block takes a tile of AX columns x AY rows of cells.
+// It first stages, for the tile and a one-cell ring around it, every value
+// its faces and rows read, boundary-mapped once per cell (star density,
+// momenta and energy, pressure, lagged momentum): coalesced loads, the maps
+// evaluated once.  Every thread then evaluates the x-face on its cell's left
+// and the y-face below it from shared memory; the tile's right x-faces and
+// top y-faces are evaluated once more by 40 threads (they belong to the
+// neighbour tiles, which store them), and the rows' right-hand sides read all
+// four faces from shared memory.  Tiles run over the face columns 0 .. nx
+// and rows 0 .. ny.
 constexpr int AX = 32, AY = 8;
+constexpr int HX = AX + 2, HY = AY + 2;  // staged cells: columns c0-1 .. c0+AX, rows j0-1 .. j0+AY
 template <int NT>
 __global__ void __launch_bounds__(NT) imex_assemble_kernel(const EcgImexMap m, const double* __restrict__ S,
                                                            const double* __restrict__ p, const double* __restrict__ K,
@@ -504,18 +583,41 @@ __global__ void __launch_bounds__(NT) imex_assemble_kernel(const EcgImexMap m, c
   __shared__ Shared sh;
   __shared__ double fx[AY][AX + 1];
   __shared__ double fy[AY + 1][AX];
+  __shared__ double t_rho[HY][HX], t_mx[HY][HX], t_my[HY][HX], t_e[HY][HX], t_p[HY][HX], t_k0[HY][HX],
+      t_k1[HY][HX];
   const int tx = threadIdx.x % AX, ty = threadIdx.x / AX;
   const int c0 = blockIdx.x * AX, j0 = blockIdx.y * AY;
   const int i = c0 + tx, j = j0 + ty;
   const int nx = m.nx, ny = m.ny;
+  for (int e = threadIdx.x; e < HX * HY; e += NT) {
+    const int ex = e % HX, ey = e / HX;
+    const int ci = c0 - 1 + ex, cj = j0 - 1 + ey;
+    const Cons c = state_b(m, S, ci, cj);
+    double k0, k1;
+    m_b(m, K, ci, cj, k0, k1);
+    t_rho[ey][ex] = c.rho;
+    t_mx[ey][ex] = c.mx;
+    t_my[ey][ex] = c.my;
+    t_e[ey][ex] = c.E;
+    t_p[ey][ex] = p_b(m, p, ci, cj);
+    t_k0[ey][ex] = k0;
+    t_k1[ey][ex] = k1;
+  }
+  __syncthreads();
+  // the face between staged cells (ax, ay) and (bx, by)
+  auto face = [&](int ax, int ay, int bx, int by, int axis) {
+    const double ql = axis == 0 ? t_k0[ay][ax] : t_k1[ay][ax];
+    const double qr = axis == 0 ? t_k0[by][bx] : t_k1[by][bx];
+    return face_math(m.gamma, t_rho[ay][ax], t_rho[by][bx], t_p[ay][ax], t_p[by][bx], ql, qr).h_hat;
+  };
   // the faces of the tile's own cells (and the domain's last face column/row)
   if (j < ny && i <= nx) {
-    const double h = face_detail(m, S, p, K, i - 1, j, i, j, 0).h_hat;
+    const double h = face(tx, ty + 1, tx + 1, ty + 1, 0);
     hx[static_cast<long long>(j) * (nx + 1) + i] = h;
     fx[ty][tx] = h;
   }
   if (i < nx && j <= ny) {
-    const double h = face_detail(m, S, p, K, i, j - 1, i, j, 1).h_hat;
+    const double h = face(tx + 1, ty, tx + 1, ty + 1, 1);
     hy[static_cast<long long>(j) * nx + i] = h;
     fy[ty][tx] = h;
   }
@@ -523,19 +625,23 @@ __global__ void __launch_bounds__(NT) imex_assemble_kernel(const EcgImexMap m, c
   // x-faces (threads 0 .. AY-1), row j0 + AY of y-faces (threads 32 .. 63)
   if (threadIdx.x < AY) {
     const int jj = j0 + threadIdx.x, ii = c0 + AX;
-    if (jj < ny && ii <= nx) fx[threadIdx.x][AX] = face_detail(m, S, p, K, ii - 1, jj, ii, jj, 0).h_hat;
+    if (jj < ny && ii <= nx) fx[threadIdx.x][AX] = face(AX, threadIdx.x + 1, AX + 1, threadIdx.x + 1, 0);
   } else if (threadIdx.x >= 32 && threadIdx.x < 32 + AX) {
-    const int ii = c0 + threadIdx.x - 32, jj = j0 + AY;
-    if (ii < nx && jj <= ny) fy[AY][threadIdx.x - 32] = face_detail(m, S, p, K, ii, jj - 1, ii, jj, 1).h_hat;
+    const int xx = threadIdx.x - 32;
+    const int ii = c0 + xx, jj = j0 + AY;
+    if (ii < nx && jj <= ny) fy[AY][xx] = face(xx + 1, AY, xx + 1, AY + 1, 1);
   }
   __syncthreads();
   long long nonfinite = 0;
   unsigned long long bmax = okey(0.0);
   if (i < nx && j < ny) {
     const double xc = 0.25 * dt * dt * idx * idx, yc = 0.25 * dt * dt * idy * idy;
+    const int sx = tx + 1, sy = ty + 1;
+    const RowData d{t_rho[sy][sx], t_mx[sy][sx],     t_my[sy][sx],     t_e[sy][sx],      t_k0[sy][sx],
+                    t_k1[sy][sx],  t_mx[sy][sx + 1], t_mx[sy][sx - 1], t_my[sy + 1][sx], t_my[sy - 1][sx]};
     int rnf;
-    const double b = rhs_row(m, S, K, fx[ty][tx + 1], fx[ty][tx], fy[ty + 1][tx], fy[ty][tx], i, j, dt, idx, idy, xc,
-                             yc, rnf);
+    const double b = rhs_math(m, d, fx[ty][tx + 1], fx[ty][tx], fy[ty + 1][tx], fy[ty][tx], i, dt, idx, idy, xc, yc,
+                              rnf);
     rhs[static_cast<long long>(j) * nx + i] = b;
     nonfinite = rnf;
     bmax = isfinite(b) ? okey(fabs(b)) : okey(kInf);
@@ -809,7 +915,7 @@ __global__ void __launch_bounds__(NT) imex_closeout_kernel(const EcgImexMap m, c
     const double pr = p[r];
     const double div = (fe - fw) * idx + (fn - fs) * idy;
     const double en = s.E - dt * div;
-    const double kin = 0.5 * (m0 * m0 + m1 * m1) / s.rho;
+    const double kin = qdiv(0.5 * (m0 * m0 + m1 * m1), s.rho);
     const double ie = en - kin;
     const double pe = gm1 * ie;
     const double res = pr / gm1 - en + kin;
@@ -896,7 +1002,7 @@ __global__ void __launch_bounds__(NT) imex_eq78_kernel(const EcgImexMap m, const
     const double rho = S[r];
     const double mm = axis == 0 ? K[r] : K[r + n];
     if (!isfinite(rho) || rho == 0.0 || !isfinite(mm)) return __longlong_as_double(0x7ff8000000000000LL);
-    return mm / rho;
+    return qdiv(mm, rho);
   };
   for (long long r = blockIdx.x * static_cast<long long>(NT) + threadIdx.x; r < n;
        r += static_cast<long long>(gridDim.x) * NT) {
@@ -982,8 +1088,8 @@ inline int blocks_for(long long n, int nt)
 inline cudaError_t imex_star(const EcgFvParams& P, const double* u, double dt, double* S, double* p, double* K,
                              EcgImexStats* st, cudaStream_t s)
 {
-  const long long n = static_cast<long long>(P.g.nx) * P.g.ny;
-  imexk::imex_star_kernel<256><<<imexk::blocks_for(n, 256), 256, 0, s>>>(P, u, dt, S, p, K, st);
+  const dim3 grid((P.g.nx + imexk::SX - 1) / imexk::SX, (P.g.ny + imexk::SY - 1) / imexk::SY);
+  imexk::imex_star_kernel<imexk::SX * imexk::SY><<<grid, imexk::SX * imexk::SY, 0, s>>>(P, u, dt, S, p, K, st);
   return cudaGetLastError();
 }
 

@@ -248,7 +248,9 @@ def test_imex_mach122_variant_against_oracle(gpu, oracle, prec):
         u1 = ctx.download()
     assert ref_d.solver_status in (1, 2)
     assert d.solver_status in (1, 2), api.solver_status_str(d.solver_status)
-    assert golden_io.state_rel_err(u1, ref_u1) <= 1e-9
+    # the mixed solve meets the same 1e-10 rule at another iterate: its state
+    # lies within a few 1e-9 of the reference's (as in test_baseline_gpu)
+    assert golden_io.state_rel_err(u1, ref_u1) <= (1e-9 if prec == "fp64" else 3e-9)
 
 
 def test_mixed_short_solves_take_the_fp64_basis(gpu):
