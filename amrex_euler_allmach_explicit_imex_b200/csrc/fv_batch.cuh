@@ -1,6 +1,9 @@
 // Batched explicit step: many independent solves of uneven grid sizes
 // advanced by one persistent launch per step.  Included inside the ecg_fast
-// namespace of stencil.cuh after fv_march.cuh (it reuses march_strip).
+// namespace of stencil.cuh after fv_march.cuh (it reuses march_strip_staged:
+// the rows of each warp strip come through the warp's shared-memory ring, as
+// in the single-grid default; 20.3 against 17.4 G cell-updates/s with the
+// rows in registers on the 64-solve bench batch).
 //
 // The solves' work is cut into tiles of WPB warp strips x H rows; tile
 // indices run over all solves (EcgBatchSolve::tile0 is the prefix sum).  A
@@ -57,12 +60,13 @@ __device__ __forceinline__ bool solve_control(EcgStepStats* __restrict__ st, con
 }
 
 template <int RK, int LIM, int H, int WPB>
-__global__ void __launch_bounds__(WPB * 32, 16 / WPB)
+__global__ void __launch_bounds__(WPB * 32, 12 / WPB)
 fv_batch_kernel(const EcgBatchSolve* __restrict__ solves, EcgStepStats* __restrict__ stats,
                 unsigned long long* __restrict__ degenerate_total, const int* __restrict__ max_step,
                 const EcgBatchCtl ctl)
 {
   __shared__ BlockRed<WPB * 32> red;
+  __shared__ march::StageRing ring[WPB];
   __shared__ EcgBatchSolve S;
   __shared__ double s_dt;
   __shared__ int s_go;
@@ -91,8 +95,8 @@ fv_batch_kernel(const EcgBatchSolve* __restrict__ solves, EcgStepStats* __restri
     march::MarchAcc acc;
     acc.init();
     if (c0 < S.p.g.nx)
-      march::march_strip<RK, LIM, true>(S.p, S.u[par], S.u[par ^ 1], c0, j0, H, s_dt, ctl.count_degenerate != 0,
-                                        acc);
+      march::march_strip_staged<RK, LIM, true>(S.p, S.u[par], S.u[par ^ 1], c0, j0, H, s_dt,
+                                               ctl.count_degenerate != 0, acc, ring[warp]);
     const int deg = block_commit<WPB * 32>(red, acc.kmax, acc.krho, acc.kp, acc.nonfinite, acc.degenerate,
                                            &stats[3 * s + ctl.acc_slot]);
     if (threadIdx.x == 0 && deg != 0) atomicAdd(&degenerate_total[s], static_cast<unsigned long long>(deg));
