@@ -368,7 +368,11 @@ const char* ecg_last_error(const ecg_ctx* ctx);
  * Element (i, j, comp) lives at base[(i - lo_x) + (j - lo_y) * jstride + comp * nstride]
  * (AMReX_Array4.H), comp in {Rho, Mx, My, E} (euler_compare_app.cpp:47).
  * Only the valid cells [0, nx) x [0, ny) are copied; ghost cells are derived
- * on the device from the boundary conditions.
+ * on the device from the boundary conditions.  A box in pinned (page-locked)
+ * memory is copied directly; a pageable one (an FArrayBox as AMReX allocates
+ * it) crosses through the context's own pinned staging copy of the state,
+ * which host threads fill or drain band by band while the previous band
+ * crosses (allocated on the first pageable call: 2 x 32 bytes a cell).
  */
 ecg_status ecg_upload_state(ecg_ctx* ctx, const double* base, int32_t lo_x, int32_t lo_y,
                             int64_t jstride, int64_t nstride);
@@ -403,7 +407,8 @@ ecg_status ecg_euler_fv_one_step(ecg_ctx* ctx, double dt, double time, int32_t* 
  * ecg_upload_state for `in` and `out`, which may be the same array): the
  * upload, the step and the download in one call, pipelined over bands of
  * rows so that band b+1 crosses to the device while band b is stepped and
- * finished bands cross back.  Pinned host memory lets the copies overlap.
+ * finished bands cross back.  Pinned host memory lets the copies overlap;
+ * pageable boxes go through the staging copy described above.
  * The context's state becomes the new state, and its fused CFL / diagnostic
  * reductions are those of `out`.  No counterpart in the reference (a drop-in
  * for its host-MultiFab call sequence upload -> euler_fv_one_step ->
