@@ -253,8 +253,7 @@ ecg_status ecg_batch_create(ecg_batch** out, int32_t nsolve, const ecg_run_confi
         (c.spatial_order != 1 && c.spatial_order != 2) || c.slope_limiter < 0 || c.slope_limiter > 2 ||
         !(c.gamma > 1.0) || !(c.prob_hi[0] > c.prob_lo[0]) || !(c.prob_hi[1] > c.prob_lo[1]))
       return ECG_ERR_BAD_ARG;
-    if (c.method != ECG_METHOD_EXPLICIT || c.riemann == ECG_RIEMANN_XIE_AM_HLLC_P ||
-        c.riemann != cfgs[0].riemann || c.slope_limiter != cfgs[0].slope_limiter ||
+    if (c.method != ECG_METHOD_EXPLICIT || c.riemann != cfgs[0].riemann || c.slope_limiter != cfgs[0].slope_limiter ||
         c.problem == ECG_PROBLEM_SHOCK_DENSITY_BUBBLE_CYLINDRICAL)
       return ECG_ERR_UNSUPPORTED;
     EcgBc bc;

@@ -199,6 +199,10 @@ cudaError_t launch_batch_step(int riemann, int limiter, int shape, const EcgBatc
     case ECG_RIEMANN_LOWMACH_HLLC:
       return batch::launch_rk<ECG_RIEMANN_LOWMACH_HLLC>(limiter, shape, solves, stats, degenerate_total, max_step,
                                                         ctl, grid, st);
+    case ECG_RIEMANN_XIE_AM_HLLC_P:
+      // the staged strip body carries the 5-face sensor along
+      return batch::launch_rk<ECG_RIEMANN_XIE_AM_HLLC_P>(limiter, shape, solves, stats, degenerate_total, max_step,
+                                                         ctl, grid, st);
     default:
       return batch::launch_rk<ECG_RIEMANN_HLLC>(limiter, shape, solves, stats, degenerate_total, max_step, ctl, grid,
                                                 st);
@@ -210,6 +214,7 @@ int batch_blocks_per_sm(int riemann, int limiter, int shape)
   switch (riemann) {
     case ECG_RIEMANN_RUSANOV: return batch::occupancy_rk<ECG_RIEMANN_RUSANOV>(limiter, shape);
     case ECG_RIEMANN_LOWMACH_HLLC: return batch::occupancy_rk<ECG_RIEMANN_LOWMACH_HLLC>(limiter, shape);
+    case ECG_RIEMANN_XIE_AM_HLLC_P: return batch::occupancy_rk<ECG_RIEMANN_XIE_AM_HLLC_P>(limiter, shape);
     default: return batch::occupancy_rk<ECG_RIEMANN_HLLC>(limiter, shape);
   }
 }

@@ -32,7 +32,7 @@ def _single(cfg, u0, steps):
         return ctx.download(), r
 
 
-@pytest.mark.parametrize("riemann", ["hllc", "rusanov", "lowmach_hllc"])
+@pytest.mark.parametrize("riemann", ["hllc", "rusanov", "lowmach_hllc", "xie_am_hllc_p"])
 def test_batch_matches_single_solves(gpu, riemann):
     cfgs, states = _batch(riemann=riemann)
     with api.Batch(cfgs) as b:
