@@ -637,7 +637,7 @@ ecg_status ecg_euler_fv_one_step(ecg_ctx* c, double dt, double time, int32_t* de
 // the context's stream and the finished bands are copied back on a third,
 // so the two copy directions and the step overlap.  Falls back to upload,
 // step, download in sequence where the step is not the column-strip kernel
-// (exact arithmetic, the HLLC-P tile kernel, exact-Dirichlet rings).
+// (exact arithmetic, HLLC-P off the staged strips, exact-Dirichlet rings).
 ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out, int32_t lo_x, int32_t lo_y,
                                       int64_t jstride, int64_t nstride, double dt, double time, int32_t* degenerate)
 {
@@ -645,8 +645,9 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
   const int nx = c->grid.nx, ny = c->grid.ny;
   if (lo_x > 0 || lo_y > 0 || jstride < nx - lo_x || nstride < jstride * (ny - lo_y)) return ECG_ERR_BAD_ARG;
   EcgFvParams p = fv_params(c, false);
+  // HLLC-P takes bands on the staged strips only (tile_y 0)
   const bool banded = c->opt.arith == ECG_ARITH_FAST && (c->tile_y == 0 || c->tile_y == 2 || c->tile_y == 3) && !c->slab() &&
-                      c->cfg.riemann != ECG_RIEMANN_XIE_AM_HLLC_P && !p.bc.ring && ny >= 32;
+                      (c->cfg.riemann != ECG_RIEMANN_XIE_AM_HLLC_P || c->tile_y == 0) && !p.bc.ring && ny >= 32;
   if (!banded) {
     ecg_status st = ecg_upload_state(c, in, lo_x, lo_y, jstride, nstride);
     if (st == ECG_OK) st = ecg_euler_fv_one_step(c, dt, time, degenerate);

@@ -559,14 +559,15 @@ inline cudaError_t launch(const EcgFvParams& p, const double* in, double* out, E
     case ECG_RIEMANN_XIE_AM_HLLC_P: {
       // Staged strips carry the 5-face sensor along, on grids whose strips
       // fill a wave of resident warps with runs of 8 rows or more (2560x640:
-      // 139 us against the tile kernel's 176 us); smaller grids, and the
-      // other variants, use the 16x16 tile kernel (Gresho 256^2: 19 us
-      // against 34 us on strips).
+      // 139 us against the tile kernel's 176 us), and for a band of rows
+      // (the pipelined host step: the tile kernel steps whole grids only);
+      // smaller grids, and the other variants, use the 16x16 tile kernel
+      // (Gresho 256^2: 19 us against 34 us on strips).
       const long long strips = (p.g.nx + kCells - 1) / kCells;
       const int rlo = p.row_hi > 0 ? p.row_lo : 0;
       const int rhi = p.row_hi > 0 && p.row_hi < p.g.ny ? p.row_hi : p.g.ny;
       const long long slots = static_cast<long long>(p.sm_count > 0 ? p.sm_count : 148) * 12;
-      if (stage && strips * ((rhi - rlo + 7) / 8) >= slots)
+      if (stage && (p.row_hi > 0 || strips * ((rhi - rlo + 7) / 8) >= slots))
         return launch_rk<ECG_RIEMANN_XIE_AM_HLLC_P, false, true>(p, in, out, stats, ctl, s);
       return fast::launch(p, in, out, stats, ctl, s);
     }

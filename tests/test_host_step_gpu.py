@@ -18,6 +18,10 @@ CASES = {
                        "geometry.is_periodic=0 1\n",
     "gresho_hllcp": "amr.n_cell=96 96\ngeometry.is_periodic=1 1\neuler.problem=gresho_vortex\neuler.vortex_center=0.5 0.5\n"
                     "euler.riemann=xie_am_hllc_p\n",
+    # HLLC-P on a grid whose device step takes the strips as well: the host
+    # step's bands run on the strips with the sensor carried across band edges
+    "bubble_hllcp": "amr.n_cell=1280 320\ngeometry.prob_hi=2 0.5\neuler.problem=shock_density_bubble_2d\n"
+                    "euler.riemann=xie_am_hllc_p\n",
 }
 
 
