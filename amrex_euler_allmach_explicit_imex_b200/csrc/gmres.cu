@@ -704,6 +704,73 @@ __device__ __forceinline__ void block_dots(const Basis<TV>& bs, const double* __
   __syncthreads();
 }
 
+// Short FP64 bases (nvec + 2 <= DG_ROWS) on blocks of more rows than
+// threads: the operator (COMB false: w = A v) or the Gram-Schmidt update
+// (COMB true: w <- w - V c, c of length nvec) and then the dot products
+// v_i . w (i < nvec), ||w||^2 and w's nonfinite flag, in ONE pass over the
+// block's rows: w is not read back, and the update's basis values serve the
+// dot products too.  Rows q and q + NT a pass and the sums in block_dots'
+// order, so the results are those of the two separate sweeps.
+template <bool COMB>
+__device__ __forceinline__ void fused_sweep_dots(const EcgPressureOp& op, Rows rw, const double* __restrict__ v,
+                                                 const Basis<double>& bs, const double* c, double* __restrict__ w,
+                                                 int nvec, const SumSink& row, double* dpart)
+{
+  constexpr int DG = DG_ROWS;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tot = nvec + 2;
+  const double* __restrict__ V = bs.V;
+  const long long n = bs.n;
+  double s[DG];
+#pragma unroll
+  for (int k = 0; k < DG; ++k) s[k] = 0.0;
+  for (int q = rw.r0 + threadIdx.x; q < rw.r1; q += 2 * NT) {
+    const bool hb = q + NT < rw.r1;
+    const int qq[2] = {q, hb ? q + NT : q};
+    double val[2];
+    double a[2][DG];
+    if (!COMB) apply_rows<double, 2>(op, v, qq, val);
+#pragma unroll
+    for (int k = 0; k < DG; ++k)
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+        a[r][k] = k < nvec ? (k < bs.K ? bs.s[k * bs.P + qq[r] - bs.r0] : __ldcg(V + static_cast<long long>(k) * n + qq[r]))
+                           : 0.0;
+    if (COMB) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) val[r] = w[qq[r]];
+#pragma unroll
+      for (int k = 0; k < DG; ++k)
+        if (k < nvec) {
+          const double ck = c[k];
+#pragma unroll
+          for (int r = 0; r < 2; ++r) val[r] = val[r] - ck * a[r][k];
+        }
+    }
+    w[qq[0]] = val[0];
+    if (hb) w[qq[1]] = val[1];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (r == 1 && !hb) break;
+#pragma unroll
+      for (int k = 0; k < DG; ++k) {
+        if (k < nvec) s[k] += a[r][k] * val[r];
+        else if (k == nvec) s[k] += val[r] * val[r];
+        else if (k == nvec + 1 && !isfinite(val[r])) s[k] = 1.0;
+      }
+    }
+  }
+  const double vs = warp_reduce_scatter<DG>(s, lane);
+  if ((lane & (32 / DG - 1)) == 0) dpart[(lane / (32 / DG)) * NW + warp] = vs;
+  __syncthreads();
+  for (int i = threadIdx.x; i < tot; i += NT) {
+    double t = 0.0;
+    for (int wv = 0; wv < NW; ++wv) t += dpart[i * NW + wv];
+    acc_add(row, i, t);
+  }
+  __syncthreads();
+}
+
 // The row sweeps of a cycle, R rows of the block at a time (R = 2 when the
 // block has more rows than threads, else 1: no duplicate loads).
 
@@ -958,10 +1025,21 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     }
     const TV* vj = V + static_cast<long long>(j) * n;
     // ---- sweep A: w = A v_j; d_i = v_i . w (i <= j); ||w||^2; nonfinite ----
-    if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
-    else sweep_spmv<TV, 1>(a.op, rw, vj, w);
-    block_dots<TV>(bs, w, rw, j + 1, true, sink(A, nred), S.dpart, pair);
-    count<TV>(S, 4.0, j + 2.0);  // w = A v_j (v_j, hx, hy, w); v_i . w (j + 1 vectors, w)
+    // (a short FP64 basis: one pass, w not read back)
+    bool fused = false;
+    if constexpr (sizeof(TV) == 8) {
+      if (wide && j + 3 <= DG_ROWS) {
+        fused_sweep_dots<false>(a.op, rw, vj, bs, nullptr, w, j + 1, sink(A, nred), S.dpart);
+        count<TV>(S, 4.0, j + 1.0);  // v_j, hx, hy, w written; j + 1 vectors
+        fused = true;
+      }
+    }
+    if (!fused) {
+      if (wide) sweep_spmv<TV, 2>(a.op, rw, vj, w);
+      else sweep_spmv<TV, 1>(a.op, rw, vj, w);
+      block_dots<TV>(bs, w, rw, j + 1, true, sink(A, nred), S.dpart, pair);
+      count<TV>(S, 4.0, j + 2.0);  // w = A v_j (v_j, hx, hy, w); v_i . w (j + 1 vectors, w)
+    }
     acc_settle(A, a.bar, nred, j + 3, nset);
     if (!grid_sync(a.bar, gen, a.spin_limit)) {
       st.timeout = 1;
@@ -991,10 +1069,21 @@ __device__ SolveState krylov(const GmresArgs& a, const double* __restrict__ bvec
     const double eta = (sizeof(TV) == 8 || reorth) ? 0.5 : 1.0e-6;
     if (!(nn2 >= eta * sw)) {
       // ---- DGKS second pass: w <- w - V d; d2_i = v_i . w; ||w||^2 ----
-      if (wide) sweep_combine<TV, true, 2>(rw, bs, S.coef, j + 1, w, w);
-      else sweep_combine<TV, true, 1>(rw, bs, S.coef, j + 1, w, w);
-      block_dots<TV>(bs, w, rw, j + 1, true, sink(A, nred), S.dpart, pair);
-      count<TV>(S, 3.0, 2.0 * (j + 1));  // w -= V d (j + 1 vectors, w twice); v_i . w again
+      // (a short FP64 basis: one pass, the basis read once)
+      bool fused2 = false;
+      if constexpr (sizeof(TV) == 8) {
+        if (wide && j + 3 <= DG_ROWS) {
+          fused_sweep_dots<true>(a.op, rw, nullptr, bs, S.coef, w, j + 1, sink(A, nred), S.dpart);
+          count<TV>(S, 2.0, j + 1.0);  // w read and written; j + 1 vectors
+          fused2 = true;
+        }
+      }
+      if (!fused2) {
+        if (wide) sweep_combine<TV, true, 2>(rw, bs, S.coef, j + 1, w, w);
+        else sweep_combine<TV, true, 1>(rw, bs, S.coef, j + 1, w, w);
+        block_dots<TV>(bs, w, rw, j + 1, true, sink(A, nred), S.dpart, pair);
+        count<TV>(S, 3.0, 2.0 * (j + 1));  // w -= V d (j + 1 vectors, w twice); v_i . w again
+      }
       acc_settle(A, a.bar, nred, j + 3, nset);
       if (!grid_sync(a.bar, gen, a.spin_limit)) {
         st.timeout = 1;
