@@ -345,7 +345,7 @@ void ecg_default_gpu_options(ecg_gpu_options* o)
   o->arith = ECG_ARITH_FAST;
   o->imex_precision = ECG_IMEX_FP64;
   o->mixed_inner_max_iter = 0;
-  o->mixed_inner_rtol = 1.0e-3;
+  o->mixed_inner_rtol = -1.0;  // chosen per system (ecg.h)
   o->mixed_max_refinements = 12;
   o->mixed_reorth = 0;
   o->mixed_min_iterations = 8;

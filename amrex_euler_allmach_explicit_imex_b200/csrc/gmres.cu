@@ -1521,6 +1521,8 @@ EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int devi
   return w;
 }
 
+bool gmres_work_resident(const EcgGmresWork* w) { return w && w->kres > 0; }
+
 void gmres_work_destroy(EcgGmresWork* w)
 {
   if (!w) return;

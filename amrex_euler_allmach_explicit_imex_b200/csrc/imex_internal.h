@@ -115,6 +115,8 @@ struct EcgGmresWork;  // gmres.cu
 
 EcgGmresWork* gmres_work_create(long long n, int max_iter, int num_sms, int device, bool mixed, std::string* err);
 void gmres_work_destroy(EcgGmresWork* w);
+// whether the solve keeps (the first of) its basis vectors in shared memory
+bool gmres_work_resident(const EcgGmresWork* w);
 // Solves A x = b from x0 (device vectors of n doubles) with the reference's
 // semantics (solve_host_sparse_gmres, imex/imex_pressure_helpers.hpp:92-217).
 // mixed: cycles on an FP32-stored Krylov basis, each opened with the true

@@ -147,7 +147,9 @@ typedef struct ecg_gpu_options {
   int32_t imex_precision;   /* ecg_imex_precision */
   int32_t mixed_inner_max_iter;  /* mixed: iterations per FP32-basis cycle (0: no limit) */
   double mixed_inner_rtol;       /* mixed: restart once the recurrence residual fell by this factor, after at
-                                    least 16 iterations of the cycle (0: never) */
+                                    least 16 iterations of the cycle (0: never; negative, the default: 1e-4
+                                    when the solve keeps its basis in shared memory, an L2-resident system,
+                                    1e-3 otherwise, where shorter cycles keep the streamed basis short) */
   int32_t mixed_max_refinements; /* mixed: cycles, each opened with the true FP64 residual */
   int32_t tile_x;           /* column-strip kernel: rows each warp marches (0: sized so the grid fills one wave) */
   int32_t tile_y;           /* explicit kernel: 0 default (column strips, x- and y-faces
