@@ -708,21 +708,31 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
     }
     return cudaSuccess;
   };
-  for (int b = 0; b < nb; ++b) {
-    const int r0 = row0(b), r1 = row0(b + 1);
-    cudaError_t e;
+  auto upload_rows = [&](int r0, int r1) -> cudaError_t {
     if (stage_in) {
       double* stage = host_stage_in(hs);
       host_stage_copy(hs, stage, const_cast<double*>(in) + off, jstride, nstride, nx, ny, r0, r1, true);
-      e = copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
-                    stage + static_cast<long long>(r0) * nx, nx, splane, r1 - r0, cudaMemcpyHostToDevice,
-                    c->up_stream);
-    } else {
-      e = copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
-                    in + off + static_cast<int64_t>(r0) * jstride, jstride, nstride, r1 - r0, cudaMemcpyHostToDevice,
-                    c->up_stream);
+      return copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
+                       stage + static_cast<long long>(r0) * nx, nx, splane, r1 - r0, cudaMemcpyHostToDevice,
+                       c->up_stream);
     }
-    if (!cuda_ok(c, e, "upload band")) return ECG_ERR_CUDA;
+    return copy_band(cur + static_cast<long long>(r0) * c->grid.pitch, c->grid.pitch, c->grid.plane,
+                     in + off + static_cast<int64_t>(r0) * jstride, jstride, nstride, r1 - r0, cudaMemcpyHostToDevice,
+                     c->up_stream);
+  };
+  // Band b's step reads rows row0(b) - 2 .. row0(b + 1) + 1, so upload chunk
+  // b carries its band's rows shifted by two, [row0(b) + 2, row0(b + 1) + 2)
+  // (the first from row 0, the last to row ny), and band b waits for chunk b
+  // alone: the downloads start one band earlier than if band b also waited
+  // for the next band's upload.  Under periodic y the first band's ghost rows
+  // are rows ny - 2 and ny - 1; they cross ahead of chunk 0 (bands are at
+  // least 16 rows, so every chunk is non-empty).
+  const bool wrap_y = p.bc.y_lo == BC_PERIODIC;
+  if (wrap_y && !cuda_ok(c, upload_rows(ny - 2, ny), "upload rows")) return ECG_ERR_CUDA;
+  for (int b = 0; b < nb; ++b) {
+    const int lo = b == 0 ? 0 : row0(b) + 2;
+    const int hi = b + 1 < nb ? row0(b + 1) + 2 : (wrap_y ? ny - 2 : ny);
+    if (!cuda_ok(c, upload_rows(lo, hi), "upload band")) return ECG_ERR_CUDA;
     if (!cuda_ok(c, cudaEventRecord(c->band_up[b], c->up_stream), "event")) return ECG_ERR_CUDA;
   }
   c->uploaded = true;
@@ -741,9 +751,8 @@ ecg_status ecg_euler_fv_one_step_host(ecg_ctx* c, const double* in, double* out,
   ctl.acc_slot = static_cast<int>((c->host_step + 1) % 3);
   ctl.reset_slot = static_cast<int>((c->host_step + 2) % 3);
   for (int b = 0; b < nb; ++b) {
-    // rows r0-2 .. r1+1 are read: this band's upload and the next one's
+    // rows r0-2 .. r1+1 are read: chunk b holds those not in earlier chunks
     if (!cuda_ok(c, cudaStreamWaitEvent(c->stream, c->band_up[b], 0), "event")) return ECG_ERR_CUDA;
-    if (b + 1 < nb && !cuda_ok(c, cudaStreamWaitEvent(c->stream, c->band_up[b + 1], 0), "event")) return ECG_ERR_CUDA;
     p.row_lo = row0(b);
     p.row_hi = row0(b + 1);
     if (!cuda_ok(c, c->ops->fv_step(p, cur, nxt, c->d_stats, ctl, c->tile_y, c->stream), "fv_step band"))

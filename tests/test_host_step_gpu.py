@@ -120,3 +120,42 @@ def test_pageable_boxes_cross_like_pinned_ones(gpu, name):
         inside = np.zeros(buf.size, dtype=bool)
         np.lib.stride_tricks.as_strided(inside[g * js + g:], shape=u0.shape, strides=(ns, js, 1))[...] = True
         assert np.isnan(buf[~inside]).all()
+
+
+# A periodic-y grid whose bands are large enough that the last upload chunk
+# lands well after the first band's step could start.
+WRAP_Y = ("amr.n_cell=1280 320\ngeometry.prob_hi=4 1\ngeometry.is_periodic=1 1\neuler.problem=gresho_vortex\n"
+          "euler.vortex_center=0.5 0.5\neuler.riemann=hllc\n")
+
+
+@pytest.mark.parametrize("memory", ["pinned", "pageable"])
+def test_host_step_reads_only_the_host_state(gpu, memory):
+    """Nothing the device buffer held before a host step reaches its result:
+    before each call the context holds a decoy (the host state rolled by half
+    the grid in y).  Under periodic y the first band's ghost rows are the
+    grid's last two rows; they must cross before that band is stepped."""
+    cfg = read_config(WRAP_Y).cfg
+    with api.Context(cfg) as ctx:
+        api.initialize_state(ctx)
+        u0 = ctx.download()
+        t, dts, states = 0.0, [], []
+        for _ in range(3):
+            dt = api.compute_euler_dt(ctx, t)
+            api.euler_fv_one_step(ctx, dt, t)
+            dts.append(dt)
+            states.append(ctx.download())
+            t += dt
+    with api.Context(cfg) as ctx:
+        if memory == "pinned":
+            a, b = _pinned(u0.shape), _pinned(u0.shape)
+            a[...] = u0
+        else:
+            a, b = np.ascontiguousarray(u0), np.empty_like(u0)
+        t = 0.0
+        for k in range(3):
+            ctx.upload(np.ascontiguousarray(np.roll(a, a.shape[1] // 2, axis=1)))
+            api.euler_fv_one_step_host(ctx, a, b, dts[k], t)
+            assert golden_io.state_rel_err(b, states[k]) <= 1e-12 * (k + 1)
+            np.testing.assert_array_equal(ctx.download(), b)
+            a, b = b, a
+            t += dts[k]
