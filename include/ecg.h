@@ -408,8 +408,11 @@ ecg_status ecg_euler_fv_one_step(ecg_ctx* ctx, double dt, double time, int32_t* 
 /* euler_fv_one_step on a HOST box (the Array4 description of
  * ecg_upload_state for `in` and `out`, which may be the same array): the
  * upload, the step and the download in one call, pipelined over bands of
- * rows so that band b+1 crosses to the device while band b is stepped and
- * finished bands cross back.  Pinned host memory lets the copies overlap;
+ * rows: each upload chunk carries the rows its band's step reads that no
+ * earlier chunk held (under periodic y the grid's last two rows, the first
+ * band's ghosts, cross first), later chunks cross while a band is stepped,
+ * and finished bands cross back.  The result depends only on `in`, never on
+ * what the context's device state held before the call.  Pinned host memory lets the copies overlap;
  * pageable boxes go through the staging copy described above.
  * The context's state becomes the new state, and its fused CFL / diagnostic
  * reductions are those of `out`.  No counterpart in the reference (a drop-in
